@@ -1,0 +1,73 @@
+/*
+ * mspai_b200 -- Matrix Market input/output and problem assembly (host, C ABI).
+ *
+ * These replace the reference's file layer: Read_mm_Matrix::Read_Matrix_File
+ * / Read_Target_File (src/Read_mm_Matrix.cpp:115-420), Pattern::
+ * Arbitrary_Pattern / Diagonal_Pattern / Matrix::To_Pattern
+ * (src/Pattern.cpp:75-139, 378-423, src/Matrix.imp:286-356) and
+ * Matrix::Write_Matrix_To_File (src/Matrix.cpp:251-340).
+ */
+#ifndef MSPAI_B200_IO_H
+#define MSPAI_B200_IO_H
+
+#include "mspai_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* A host CSC matrix owned by the library (free with mspai_matrix_free). */
+typedef struct {
+    int32_t nrows, ncols;
+    int64_t nnz;
+    int64_t* colptr;
+    int32_t* rowidx;
+    double* values;  /* NULL for a pattern file */
+    int32_t symmetric; /* the file was stored symmetric (expanded on read) */
+} mspai_matrix;
+
+/* View of an owned matrix as a mspai_csc (host memory). */
+mspai_csc mspai_matrix_view(const mspai_matrix* m);
+
+void mspai_matrix_free(mspai_matrix* m);
+
+/*
+ * Reads a Matrix Market coordinate file (real, integer or pattern; general or
+ * symmetric; symmetric files are expanded).  Entries are sorted by column and
+ * row; duplicate entries are summed.  Returns MSPAI_ERR_IO / MSPAI_ERR_INPUT
+ * with a message in msg on failure.
+ */
+int mspai_mm_read(const char* path, mspai_matrix* out, char* msg, int32_t msg_len);
+
+/*
+ * Writes M in the reference's output format: "%%MatrixMarket matrix
+ * coordinate real general", "m n nnz", then one "row col<sp>value" line per
+ * entry, 1-based, value "%.13e" preceded by one space if negative and two
+ * otherwise (src/Matrix.cpp:290-312).
+ */
+int mspai_mm_write(const char* path, const mspai_csc* M, char* msg, int32_t msg_len);
+
+/*
+ * Builds C = [A; rho * Ce] (probing rows appended at n..n+p-1, values
+ * scaled by rho as src/Read_mm_Matrix.cpp:566-577) and the target
+ * B = [I; rho * Be] (src/Read_mm_Matrix.cpp:601-667).  Ce and Be are p x n;
+ * either may be NULL (no probing: C = A and B = I).  Outputs are owned.
+ */
+int mspai_probing_assemble(const mspai_csc* A, const mspai_csc* Ce, const mspai_csc* Be,
+                           double rho, mspai_matrix* C_out, mspai_matrix* B_out, char* msg,
+                           int32_t msg_len);
+
+/*
+ * Start patterns: kind 1 = diagonal (Diagonal_Pattern), kind 2 = the pattern
+ * of the first n rows of C (To_Pattern with probing rows omitted).
+ */
+int mspai_pattern_generate(const mspai_csc* C, int32_t kind, mspai_matrix* P_out);
+
+/* CSR row structure of the first nrows_keep rows of C, as a CSC of C^T. */
+int mspai_row_structure(const mspai_csc* C, int32_t nrows_keep, mspai_matrix* R_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MSPAI_B200_IO_H */

@@ -1,0 +1,320 @@
+"""Python interface of the B200 MSPAI setup.
+
+It mirrors the reference's setup entry points: ``Options`` carries the
+command-line options of the reference (src/Command_Line.cpp:192-225,
+src/imspai.cpp:57-218) with the reference's checks; ``Handle.setup`` is
+``Spai<double>::SPAI_Algorithm`` (src/Spai.imp:33-191) on plain CSC arrays;
+``mspai`` is the serial command line ``mspai A P|-1|-2 B|-1 [options]``
+(probing rows assembled as Read_mm_Matrix does, src/Read_mm_Matrix.cpp:115-420).
+
+Matrices are scipy.sparse (host memory) or ``DeviceCSC`` (torch CUDA tensors,
+already resident on the GPU).  All compute runs in the CUDA library; there is
+no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+from typing import Optional, Tuple, Union
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _lib
+from ._lib import MEM_DEVICE, MEM_HOST, MspaiError, mspai_csc, mspai_params, mspai_stats
+
+
+@dataclasses.dataclass
+class Options:
+    """Reference options (names and defaults of the reference's command line)."""
+    ep: float = 0.4
+    mn: int = 5
+    ns: int = 5
+    um: int = 1
+    hs: int = 6
+    cs: int = 0
+    qr: int = 0
+    ch: int = 0
+    fg: float = 0.3
+    pk: int = 0
+    pm: int = 0
+    schur: int = 0
+    rho: float = 1.0
+    bs: int = 1
+    target: int = 1
+    probing: int = 0
+    prec: str = "mixed"        # "fp64" or "mixed"
+    refine: int = 2
+    batched: bool = True
+    verbose: int = 0
+
+    def to_c(self) -> mspai_params:
+        p = mspai_params()
+        _lib.load().mspai_default_params(ctypes.byref(p))
+        for f in ("ep", "mn", "ns", "um", "hs", "cs", "qr", "ch", "fg", "pk", "pm", "schur",
+                  "rho", "bs", "target", "probing", "refine", "verbose"):
+            setattr(p, f, getattr(self, f))
+        p.prec = _lib.PREC_FP64 if self.prec == "fp64" else _lib.PREC_MIXED
+        p.batched = 1 if self.batched else 0
+        return p
+
+    def validate(self) -> None:
+        """Raises ValueError with the reference's message for invalid options."""
+        buf = ctypes.create_string_buffer(1024)
+        p = self.to_c()
+        rc = _lib.load().mspai_validate_params(ctypes.byref(p), buf, len(buf))
+        if rc != _lib.MSPAI_OK:
+            raise ValueError(buf.value.decode())
+
+
+class DeviceCSC:
+    """A CSC matrix resident on the GPU (torch tensors: int64 colptr, int32
+    rowidx, float64 values or None for a pattern)."""
+
+    def __init__(self, nrows: int, ncols: int, colptr, rowidx, values=None):
+        self.nrows, self.ncols = int(nrows), int(ncols)
+        self.colptr, self.rowidx, self.values = colptr, rowidx, values
+
+    @property
+    def nnz(self) -> int:
+        return int(self.rowidx.numel())
+
+    @staticmethod
+    def from_scipy(M: sp.spmatrix, device="cuda", pattern: bool = False) -> "DeviceCSC":
+        import torch
+        M = _canon(M)
+        cp = torch.from_numpy(np.asarray(M.indptr, dtype=np.int64)).to(device)
+        ri = torch.from_numpy(np.asarray(M.indices, dtype=np.int32)).to(device)
+        v = None if pattern else torch.from_numpy(np.asarray(M.data, dtype=np.float64)).to(device)
+        return DeviceCSC(M.shape[0], M.shape[1], cp, ri, v)
+
+
+def _canon(M: sp.spmatrix) -> sp.csc_matrix:
+    M = sp.csc_matrix(M)
+    if not M.has_sorted_indices:
+        M = M.copy()
+        M.sort_indices()
+    return M
+
+
+class _Staged:
+    """Keeps the numpy arrays behind a host mspai_csc alive."""
+
+    def __init__(self, M, pattern: bool):
+        if isinstance(M, DeviceCSC):
+            self.keep = (M.colptr, M.rowidx, M.values)
+            self.c = mspai_csc(M.nrows, M.ncols, M.nnz, M.colptr.data_ptr(), M.rowidx.data_ptr(),
+                               None if (pattern or M.values is None) else M.values.data_ptr(),
+                               MEM_DEVICE)
+            return
+        M = _canon(M)
+        cp = np.ascontiguousarray(M.indptr, dtype=np.int64)
+        ri = np.ascontiguousarray(M.indices, dtype=np.int32)
+        vv = None if pattern else np.ascontiguousarray(M.data, dtype=np.float64)
+        self.keep = (cp, ri, vv)
+        self.c = mspai_csc(M.shape[0], M.shape[1], M.nnz, cp.ctypes.data, ri.ctypes.data,
+                           None if vv is None else vv.ctypes.data, MEM_HOST)
+
+
+MatrixLike = Union[sp.spmatrix, DeviceCSC]
+
+
+class Handle:
+    """One setup context on one GPU (wraps mspai_create / mspai_free)."""
+
+    def __init__(self, device: int = 0, stream: Optional[int] = None):
+        self._lib = _lib.load()
+        h = ctypes.c_void_p()
+        rc = self._lib.mspai_create(ctypes.byref(h), int(device), stream)
+        if rc != _lib.MSPAI_OK:
+            raise MspaiError(rc, "mspai_create failed (is a CUDA device visible?)")
+        self._h = h
+        self.n = 0
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.mspai_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int) -> None:
+        if rc != _lib.MSPAI_OK:
+            msg = self._lib.mspai_last_error(self._h).decode(errors="replace")
+            raise MspaiError(rc, msg)
+
+    def setup(self, C: MatrixLike, P: MatrixLike, B: Optional[MatrixLike] = None,
+              UP: Optional[MatrixLike] = None, C_rows: Optional[MatrixLike] = None,
+              options: Optional[Options] = None) -> None:
+        """Spai<double>::SPAI_Algorithm on CSC inputs (see mspai_setup)."""
+        opts = options or Options()
+        p = opts.to_c()
+        sc = _Staged(C, False)
+        sp_ = _Staged(P, True)
+        sb = _Staged(B, False) if B is not None else None
+        su = _Staged(UP, True) if UP is not None else None
+        sr = _Staged(C_rows, True) if C_rows is not None else None
+        rc = self._lib.mspai_setup(self._h, ctypes.byref(sc.c),
+                                   ctypes.byref(sr.c) if sr else None,
+                                   ctypes.byref(sb.c) if sb else None, ctypes.byref(sp_.c),
+                                   ctypes.byref(su.c) if su else None, ctypes.byref(p))
+        self._check(rc)
+        self.n = sc.c.ncols
+
+    def nnz(self) -> int:
+        v = ctypes.c_int64()
+        self._check(self._lib.mspai_result_nnz(self._h, ctypes.byref(v)))
+        return int(v.value)
+
+    def result(self) -> sp.csc_matrix:
+        """M as a host scipy CSC matrix."""
+        nnz = self.nnz()
+        cp = np.zeros(self.n + 1, dtype=np.int64)
+        ri = np.zeros(max(nnz, 1), dtype=np.int32)
+        vv = np.zeros(max(nnz, 1), dtype=np.float64)
+        self._check(self._lib.mspai_result_copy(self._h, cp.ctypes.data, ri.ctypes.data,
+                                                vv.ctypes.data, MEM_HOST))
+        return sp.csc_matrix((vv[:nnz], ri[:nnz], cp), shape=(self.n, self.n))
+
+    def result_into(self, colptr=None, rowidx=None, values=None, device: bool = False) -> None:
+        """Copies M into caller arrays (numpy, or torch CUDA tensors if device)."""
+        def ptr(a):
+            if a is None:
+                return None
+            return a.data_ptr() if device else a.ctypes.data
+        self._check(self._lib.mspai_result_copy(self._h, ptr(colptr), ptr(rowidx), ptr(values),
+                                                MEM_DEVICE if device else MEM_HOST))
+
+    def column_info(self) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        res = np.zeros(self.n, dtype=np.float64)
+        steps = np.zeros(self.n, dtype=np.int32)
+        status = np.zeros(self.n, dtype=np.int32)
+        self._check(self._lib.mspai_column_info(self._h, res.ctypes.data, steps.ctypes.data,
+                                                status.ctypes.data))
+        return res, steps, status
+
+    def stats(self) -> dict:
+        s = mspai_stats()
+        self._check(self._lib.mspai_get_stats(self._h, ctypes.byref(s)))
+        return {
+            "columns": s.columns, "ls_solves": s.ls_solves, "nnz_m": s.nnz_m,
+            "singular_columns": s.singular_columns, "capacity_columns": s.capacity_columns,
+            "bucket_columns": list(s.bucket_columns)[:3], "flops": s.flops,
+            "flops_dense": s.flops_dense, "gather_bytes": s.gather_bytes,
+            "setup_ms": s.setup_ms, "kernel_ms": list(s.kernel_ms)[:3],
+        }
+
+    def adjoint(self, C: MatrixLike, B: Optional[MatrixLike] = None,
+                gbar: Optional[np.ndarray] = None):
+        """Gradient of ||C M - B||_F^2 + gbar . M w.r.t. the nonzeros of C and B.
+
+        Returns (dC, dB, loss) as host arrays in C's / B's nonzero order."""
+        sc = _Staged(C, False)
+        sb = _Staged(B, False) if B is not None else None
+        dC = np.zeros(max(sc.c.nnz, 1), dtype=np.float64)
+        dB = np.zeros(max(sb.c.nnz, 1), dtype=np.float64) if sb else None
+        g = None
+        if gbar is not None:
+            g = np.ascontiguousarray(gbar, dtype=np.float64)
+        loss = ctypes.c_double()
+        rc = self._lib.mspai_adjoint(self._h, ctypes.byref(sc.c),
+                                     ctypes.byref(sb.c) if sb else None,
+                                     None if g is None else g.ctypes.data, dC.ctypes.data,
+                                     None if dB is None else dB.ctypes.data,
+                                     ctypes.byref(loss), MEM_HOST)
+        self._check(rc)
+        return dC[:sc.c.nnz], (dB[:sb.c.nnz] if dB is not None else None), float(loss.value)
+
+
+def assemble_probing(A: sp.spmatrix, Ce: Optional[sp.spmatrix], Be: Optional[sp.spmatrix],
+                     rho: float) -> Tuple[sp.csc_matrix, sp.csc_matrix]:
+    """C = [A; rho Ce], B = [I; rho Be] (mspai_probing_assemble)."""
+    lib = _lib.load()
+    sa = _Staged(A, False)
+    sce = _Staged(sp.csc_matrix(Ce), False) if Ce is not None else None
+    sbe = _Staged(sp.csc_matrix(Be), False) if Be is not None else None
+    Cm, Bm = _lib.mspai_matrix(), _lib.mspai_matrix()
+    buf = ctypes.create_string_buffer(512)
+    rc = lib.mspai_probing_assemble(ctypes.byref(sa.c), ctypes.byref(sce.c) if sce else None,
+                                    ctypes.byref(sbe.c) if sbe else None, float(rho),
+                                    ctypes.byref(Cm), ctypes.byref(Bm), buf, len(buf))
+    if rc != _lib.MSPAI_OK:
+        raise MspaiError(rc, buf.value.decode())
+    try:
+        return _owned_to_scipy(Cm), _owned_to_scipy(Bm)
+    finally:
+        lib.mspai_matrix_free(ctypes.byref(Cm))
+        lib.mspai_matrix_free(ctypes.byref(Bm))
+
+
+def _owned_to_scipy(m) -> sp.csc_matrix:
+    n, nnz = m.ncols, m.nnz
+    cp = np.ctypeslib.as_array(m.colptr, shape=(n + 1,)).copy()
+    ri = np.ctypeslib.as_array(m.rowidx, shape=(max(nnz, 1),))[:nnz].copy()
+    if m.values:
+        vv = np.ctypeslib.as_array(m.values, shape=(max(nnz, 1),))[:nnz].copy()
+    else:
+        vv = np.ones(nnz)
+    return sp.csc_matrix((vv, ri, cp), shape=(m.nrows, n))
+
+
+def read_mm(path: str) -> sp.csc_matrix:
+    """Matrix Market reader of the library (mspai_mm_read)."""
+    lib = _lib.load()
+    m = _lib.mspai_matrix()
+    buf = ctypes.create_string_buffer(512)
+    rc = lib.mspai_mm_read(path.encode(), ctypes.byref(m), buf, len(buf))
+    if rc != _lib.MSPAI_OK:
+        raise MspaiError(rc, buf.value.decode())
+    try:
+        return _owned_to_scipy(m)
+    finally:
+        lib.mspai_matrix_free(ctypes.byref(m))
+
+
+def write_mm(path: str, M: sp.spmatrix) -> None:
+    """Writes M in the reference's output format (mspai_mm_write)."""
+    lib = _lib.load()
+    s = _Staged(M, False)
+    buf = ctypes.create_string_buffer(512)
+    rc = lib.mspai_mm_write(path.encode(), ctypes.byref(s.c), buf, len(buf))
+    if rc != _lib.MSPAI_OK:
+        raise MspaiError(rc, buf.value.decode())
+
+
+def start_pattern(C: sp.spmatrix, kind: Union[int, str]) -> sp.csc_matrix:
+    """-1 / "diag": diagonal pattern; -2 / "A": pattern of C's first n rows."""
+    k = {"diag": 1, -1: 1, 1: 1, "A": 2, -2: 2, 2: 2}[kind]
+    lib = _lib.load()
+    s = _Staged(C, False)
+    m = _lib.mspai_matrix()
+    rc = lib.mspai_pattern_generate(ctypes.byref(s.c), k, ctypes.byref(m))
+    if rc != _lib.MSPAI_OK:
+        raise MspaiError(rc, "pattern generation failed")
+    try:
+        return _owned_to_scipy(m)
+    finally:
+        lib.mspai_matrix_free(ctypes.byref(m))
+
+
+def mspai(A: sp.spmatrix, pattern: Union[int, str, sp.spmatrix] = -1,
+          target: Optional[sp.spmatrix] = None, Ce: Optional[sp.spmatrix] = None,
+          Be: Optional[sp.spmatrix] = None, UP: Optional[sp.spmatrix] = None,
+          options: Optional[Options] = None, device: int = 0):
+    """The serial command line as a function: returns (M, handle)."""
+    opts = dataclasses.replace(options or Options())
+    opts.probing = 1 if (Ce is not None or Be is not None) else 0
+    opts.target = 1 if target is None else 0
+    opts.validate()
+    C, B = assemble_probing(A, Ce, Be, opts.rho)
+    Bin = B if opts.probing else None
+    if target is not None:
+        Bin = target
+    P = pattern if sp.issparse(pattern) else start_pattern(C, pattern)
+    h = Handle(device)
+    h.setup(C, P, B=Bin, UP=UP, options=opts)
+    return h.result(), h

@@ -1,0 +1,729 @@
+// Host engine behind the C ABI of include/mspai_b200.h.
+//
+// mspai_setup replaces Spai<double>::SPAI_Algorithm (reference
+// src/Spai.imp:33-191): it stages the inputs in device memory, plans and bins
+// the columns by problem size, runs the bucket kernels, and assembles M's CSC
+// on the device.  Everything a setup allocates is owned by the handle and
+// reused by the next setup of the same or a smaller size.
+#include "mspai_b200.h"
+#include "host_util.h"
+#include "spai_kernels.h"
+#include "spai_solve.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+
+using mspai::BucketRule;
+using mspai::Caps;
+using mspai::Output;
+using mspai::Problem;
+
+constexpr int kBuckets = 3;
+
+// A device buffer that grows on demand.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t want)
+    {
+        if (want <= bytes && p)
+            return cudaSuccess;
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        size_t alloc = std::max<size_t>(want, 256);
+        cudaError_t e = cudaMalloc(&p, alloc);
+        if (e == cudaSuccess)
+            bytes = alloc;
+        return e;
+    }
+    void release()
+    {
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    template <class T>
+    T* as() const
+    {
+        return static_cast<T*>(p);
+    }
+};
+
+}  // namespace
+
+struct mspai_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+    // staged inputs
+    DevBuf cptr, cidx, cval, rptr, rcol, bptr, bidx, bval, pptr, pidx, upptr, upidx;
+    // planning
+    DevBuf E, nk, lists, counters, scan_tmp, cap_len, cap_ptr;
+    // outputs
+    DevBuf oidx, oval, olen, res, steps, status, work;
+    DevBuf mptr, midx, mval;  // final M
+    DevBuf scratch;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t evb[2 * kBuckets] = {};
+    // result description
+    int n = 0;
+    int64_t nnz_m = 0;
+    bool have_result = false;
+    bool fixed_pattern = true;
+    const int64_t* res_ptr = nullptr;
+    const int32_t* res_idx = nullptr;
+    const double* res_val = nullptr;
+    mspai_stats stats{};
+    mspai_params last_params{};
+};
+
+static int set_err(mspai_handle* h, int code, const char* fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (h)
+        h->err = buf;
+    return code;
+}
+
+#define CUDA_TRY(h, expr)                                                                        \
+    do {                                                                                         \
+        cudaError_t _e = (expr);                                                                 \
+        if (_e != cudaSuccess)                                                                   \
+            return set_err((h), _e == cudaErrorMemoryAllocation ? MSPAI_ERR_ALLOC : MSPAI_ERR_CUDA, \
+                           "%s: %s (%s:%d)", #expr, cudaGetErrorString(_e), __FILE__, __LINE__); \
+    } while (0)
+
+// Stages an array on the device: borrows device pointers, copies host ones.
+template <class T>
+static cudaError_t stage(DevBuf& buf, const T* src, size_t count, int mem, cudaStream_t st,
+                         const T** out)
+{
+    if (src == nullptr || count == 0) {
+        *out = nullptr;
+        if (count == 0 && src != nullptr) {
+            cudaError_t e = buf.ensure(sizeof(T));
+            *out = buf.as<T>();
+            return e;
+        }
+        return cudaSuccess;
+    }
+    if (mem == MSPAI_MEM_DEVICE) {
+        *out = src;
+        return cudaSuccess;
+    }
+    cudaError_t e = buf.ensure(count * sizeof(T));
+    if (e != cudaSuccess)
+        return e;
+    e = cudaMemcpyAsync(buf.p, src, count * sizeof(T), cudaMemcpyHostToDevice, st);
+    *out = buf.as<T>();
+    return e;
+}
+
+template <class T>
+static cudaError_t fetch(std::vector<T>& dst, const T* src, size_t count, int mem, cudaStream_t st)
+{
+    dst.resize(count);
+    if (count == 0)
+        return cudaSuccess;
+    if (mem == MSPAI_MEM_HOST) {
+        std::memcpy(dst.data(), src, count * sizeof(T));
+        return cudaSuccess;
+    }
+    cudaError_t e = cudaMemcpyAsync(dst.data(), src, count * sizeof(T), cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess)
+        return e;
+    return cudaStreamSynchronize(st);
+}
+
+extern "C" {
+
+const char* mspai_version(void) { return "mspai_b200 0.1"; }
+
+int mspai_create(mspai_handle** out, int32_t device, void* stream)
+{
+    if (!out)
+        return MSPAI_ERR_PARAM;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+        cudaGetLastError();
+        return MSPAI_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= count)
+        return MSPAI_ERR_NO_DEVICE;
+    mspai_handle* h = new (std::nothrow) mspai_handle();
+    if (!h)
+        return MSPAI_ERR_ALLOC;
+    h->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        delete h;
+        return MSPAI_ERR_CUDA;
+    }
+    if (stream) {
+        h->stream = static_cast<cudaStream_t>(stream);
+    }
+    else {
+        if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete h;
+            return MSPAI_ERR_CUDA;
+        }
+        h->own_stream = true;
+    }
+    cudaEventCreate(&h->ev0);
+    cudaEventCreate(&h->ev1);
+    for (auto& e : h->evb)
+        cudaEventCreate(&e);
+    *out = h;
+    return MSPAI_OK;
+}
+
+void mspai_free(mspai_handle* h)
+{
+    if (!h)
+        return;
+    cudaSetDevice(h->device);
+    if (h->stream)
+        cudaStreamSynchronize(h->stream);
+    DevBuf* bufs[] = {&h->cptr, &h->cidx, &h->cval, &h->rptr, &h->rcol, &h->bptr, &h->bidx,
+                      &h->bval, &h->pptr, &h->pidx, &h->upptr, &h->upidx, &h->E, &h->nk,
+                      &h->lists, &h->counters, &h->scan_tmp, &h->cap_len, &h->cap_ptr, &h->oidx,
+                      &h->oval, &h->olen, &h->res, &h->steps, &h->status, &h->work, &h->mptr,
+                      &h->midx, &h->mval, &h->scratch};
+    for (DevBuf* b : bufs)
+        b->release();
+    if (h->ev0)
+        cudaEventDestroy(h->ev0);
+    if (h->ev1)
+        cudaEventDestroy(h->ev1);
+    for (auto& e : h->evb)
+        if (e)
+            cudaEventDestroy(e);
+    if (h->own_stream && h->stream)
+        cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+const char* mspai_last_error(mspai_handle* h)
+{
+    return h ? h->err.c_str() : "null handle";
+}
+
+static int check_csc(mspai_handle* h, const mspai_csc* m, const char* name, bool need_values)
+{
+    if (!m->colptr || (m->nnz > 0 && !m->rowidx))
+        return set_err(h, MSPAI_ERR_INPUT, "%s: missing arrays", name);
+    if (need_values && m->nnz > 0 && !m->values)
+        return set_err(h, MSPAI_ERR_INPUT, "%s: missing values", name);
+    if (m->nrows < 0 || m->ncols < 0 || m->nnz < 0)
+        return set_err(h, MSPAI_ERR_INPUT, "%s: negative size", name);
+    if (m->mem != MSPAI_MEM_HOST && m->mem != MSPAI_MEM_DEVICE)
+        return set_err(h, MSPAI_ERR_INPUT, "%s: bad memory kind", name);
+    if (m->mem == MSPAI_MEM_HOST) {
+        if (m->colptr[0] != 0 || m->colptr[m->ncols] != m->nnz)
+            return set_err(h, MSPAI_ERR_INPUT, "%s: column pointers do not match nnz", name);
+        for (int c = 0; c < m->ncols; c++) {
+            if (m->colptr[c + 1] < m->colptr[c])
+                return set_err(h, MSPAI_ERR_INPUT, "%s: column pointers decrease", name);
+            for (int64_t p = m->colptr[c]; p < m->colptr[c + 1]; p++) {
+                const int r = m->rowidx[p];
+                if (r < 0 || r >= m->nrows)
+                    return set_err(h, MSPAI_ERR_INPUT, "%s: row index %d out of range in column %d",
+                                   name, r, c);
+                if (p > m->colptr[c] && m->rowidx[p - 1] >= r)
+                    return set_err(h, MSPAI_ERR_INPUT,
+                                   "%s: row indices not sorted/unique in column %d", name, c);
+            }
+        }
+    }
+    return MSPAI_OK;
+}
+
+int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, const mspai_csc* B,
+                const mspai_csc* P, const mspai_csc* UP, const mspai_params* prm)
+{
+    if (!h)
+        return MSPAI_ERR_STATE;
+    h->err.clear();
+    h->have_result = false;
+    if (!C || !P || !prm)
+        return set_err(h, MSPAI_ERR_PARAM, "C, P and params are required");
+    char msg[1024];
+    int rc = mspai_validate_params(prm, msg, sizeof(msg));
+    if (rc != MSPAI_OK)
+        return set_err(h, rc, "%s", msg);
+    if (prm->bs != 1)
+        return set_err(h, MSPAI_ERR_PARAM, "block SPAI (-bs %d) is served by mspai_setup_block",
+                       prm->bs);
+    const int n = C->ncols;
+    if ((rc = check_csc(h, C, "C", true)) != MSPAI_OK)
+        return rc;
+    if ((rc = check_csc(h, P, "P", false)) != MSPAI_OK)
+        return rc;
+    if (C->nrows < n)
+        return set_err(h, MSPAI_ERR_INPUT, "C has fewer rows (%d) than columns (%d)", C->nrows, n);
+    if (P->ncols != n || P->nrows != n)
+        return set_err(h, MSPAI_ERR_INPUT, "pattern must be %d x %d", n, n);
+    if (B) {
+        if ((rc = check_csc(h, B, "B", true)) != MSPAI_OK)
+            return rc;
+        if (B->ncols != n || B->nrows != C->nrows)
+            return set_err(h, MSPAI_ERR_INPUT, "target must be %d x %d", C->nrows, n);
+    }
+    if (UP) {
+        if ((rc = check_csc(h, UP, "UP", false)) != MSPAI_OK)
+            return rc;
+        if (UP->ncols != n || UP->nrows != n)
+            return set_err(h, MSPAI_ERR_INPUT, "upper pattern must be %d x %d", n, n);
+    }
+    // empty columns of C: the reference rejects them (src/Read_mm_Matrix.cpp:745-751)
+    if (C->mem == MSPAI_MEM_HOST) {
+        for (int c = 0; c < n; c++)
+            if (C->colptr[c + 1] == C->colptr[c])
+                return set_err(h, MSPAI_ERR_INPUT,
+                               "Matrix is singular: column %d of C is empty", c);
+    }
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    const bool adaptive = prm->ns > 0 && prm->mn > 0;
+    h->fixed_pattern = !adaptive;
+    h->n = n;
+
+    // ---- stage inputs
+    Problem pb{};
+    pb.n = n;
+    pb.nrows = C->nrows;
+    CUDA_TRY(h, stage(h->cptr, C->colptr, n + 1, C->mem, st, &pb.cptr));
+    CUDA_TRY(h, stage(h->cidx, C->rowidx, C->nnz, C->mem, st, &pb.cidx));
+    CUDA_TRY(h, stage(h->cval, C->values, C->nnz, C->mem, st, &pb.cval));
+    CUDA_TRY(h, stage(h->pptr, P->colptr, n + 1, P->mem, st, &pb.pptr));
+    CUDA_TRY(h, stage(h->pidx, P->rowidx, P->nnz, P->mem, st, &pb.pidx));
+    if (B) {
+        CUDA_TRY(h, stage(h->bptr, B->colptr, n + 1, B->mem, st, &pb.bptr));
+        CUDA_TRY(h, stage(h->bidx, B->rowidx, B->nnz, B->mem, st, &pb.bidx));
+        CUDA_TRY(h, stage(h->bval, B->values, B->nnz, B->mem, st, &pb.bval));
+    }
+    if (UP) {
+        CUDA_TRY(h, stage(h->upptr, UP->colptr, n + 1, UP->mem, st, &pb.upptr));
+        CUDA_TRY(h, stage(h->upidx, UP->rowidx, UP->nnz, UP->mem, st, &pb.upidx));
+    }
+    int max_row_nnz = 0, max_col_nnz = 0;
+    if (adaptive) {
+        std::vector<int64_t> rp;
+        std::vector<int32_t> rc2;
+        if (C_rows) {
+            if ((rc = check_csc(h, C_rows, "C_rows", false)) != MSPAI_OK)
+                return rc;
+            CUDA_TRY(h, stage(h->rptr, C_rows->colptr, C_rows->ncols + 1, C_rows->mem, st, &pb.rptr));
+            CUDA_TRY(h, stage(h->rcol, C_rows->rowidx, C_rows->nnz, C_rows->mem, st, &pb.rcol));
+            CUDA_TRY(h, fetch(rp, C_rows->colptr, C_rows->ncols + 1, C_rows->mem, st));
+        }
+        else {
+            std::vector<int64_t> cp;
+            std::vector<int32_t> ci;
+            CUDA_TRY(h, fetch(cp, C->colptr, n + 1, C->mem, st));
+            CUDA_TRY(h, fetch(ci, C->rowidx, C->nnz, C->mem, st));
+            mspai_host::csc_row_structure(n, cp.data(), ci.data(), n, rp, rc2);
+            const int64_t* rpp = nullptr;
+            const int32_t* rcp = nullptr;
+            CUDA_TRY(h, stage(h->rptr, rp.data(), rp.size(), MSPAI_MEM_HOST, st, &rpp));
+            CUDA_TRY(h, stage(h->rcol, rc2.data(), rc2.size(), MSPAI_MEM_HOST, st, &rcp));
+            pb.rptr = rpp;
+            pb.rcol = rcp;
+            CUDA_TRY(h, cudaStreamSynchronize(st));  // host vectors go out of scope
+        }
+        for (size_t i = 0; i + 1 < rp.size(); i++)
+            max_row_nnz = std::max<int>(max_row_nnz, static_cast<int>(rp[i + 1] - rp[i]));
+    }
+    pb.ep = prm->ep;
+    pb.mn = prm->mn;
+    pb.ns = adaptive ? prm->ns : 0;
+    pb.um = prm->um;
+    const bool mixed = prm->prec == MSPAI_PREC_MIXED && prm->batched;
+    pb.refine = mixed ? std::max(0, prm->refine) : 0;
+    const int elem = mixed ? 4 : 8;
+
+    // ---- time the device part of the setup
+    CUDA_TRY(h, cudaEventRecord(h->ev0, st));
+
+    // max column nnz of C (growth bound of the entry count)
+    CUDA_TRY(h, h->counters.ensure(64 * sizeof(int32_t)));
+    int32_t* dcnt = h->counters.as<int32_t>();
+    CUDA_TRY(h, mspai::launch_max_len(pb.cptr, n, dcnt + 16, st));
+    CUDA_TRY(h, cudaMemcpyAsync(&max_col_nnz, dcnt + 16, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+
+    // ---- output capacity
+    Output out{};
+    const int grow_n = adaptive ? prm->mn * prm->ns : 0;
+    CUDA_TRY(h, h->olen.ensure(sizeof(int32_t) * std::max(n, 1)));
+    CUDA_TRY(h, h->res.ensure(sizeof(double) * std::max(n, 1)));
+    CUDA_TRY(h, h->steps.ensure(sizeof(int32_t) * std::max(n, 1)));
+    CUDA_TRY(h, h->status.ensure(sizeof(int32_t) * std::max(n, 1)));
+    CUDA_TRY(h, h->work.ensure(sizeof(double) * 3 * std::max(n, 1)));
+    CUDA_TRY(h, cudaMemsetAsync(h->work.p, 0, sizeof(double) * 3 * std::max(n, 1), st));
+    CUDA_TRY(h, h->scan_tmp.ensure(sizeof(int64_t) * ((n + 1023) / 1024 + 2)));
+    int64_t cap_total = P->nnz;
+    if (adaptive) {
+        CUDA_TRY(h, h->cap_len.ensure(sizeof(int32_t) * std::max(n, 1)));
+        CUDA_TRY(h, h->cap_ptr.ensure(sizeof(int64_t) * (n + 1)));
+        CUDA_TRY(h, mspai::launch_capacity_len(pb.pptr, n, grow_n, h->cap_len.as<int32_t>(), st));
+        CUDA_TRY(h, mspai::launch_scan_lengths(h->cap_len.as<int32_t>(), n, h->cap_ptr.as<int64_t>(),
+                                               h->scan_tmp.as<int64_t>(), st));
+        cap_total = P->nnz + static_cast<int64_t>(grow_n) * n;
+        CUDA_TRY(h, h->oidx.ensure(sizeof(int32_t) * std::max<int64_t>(cap_total, 1)));
+        out.optr = h->cap_ptr.as<int64_t>();
+        out.oidx = h->oidx.as<int32_t>();
+        out.write_idx = 1;
+    }
+    else {
+        out.optr = pb.pptr;
+        out.oidx = nullptr;
+        out.write_idx = 0;
+    }
+    CUDA_TRY(h, h->oval.ensure(sizeof(double) * std::max<int64_t>(cap_total, 1)));
+    out.oval = h->oval.as<double>();
+    out.olen = h->olen.as<int32_t>();
+    out.res = h->res.as<double>();
+    out.steps = h->steps.as<int32_t>();
+    out.status = h->status.as<int32_t>();
+    out.work = h->work.as<double>();
+
+    // ---- plan and bucket
+    CUDA_TRY(h, h->E.ensure(sizeof(int32_t) * std::max(n, 1)));
+    CUDA_TRY(h, h->nk.ensure(sizeof(int32_t) * std::max(n, 1)));
+    CUDA_TRY(h, h->lists.ensure(sizeof(int32_t) * static_cast<size_t>(kBuckets) * std::max(n, 1)));
+    CUDA_TRY(h, mspai::launch_plan(pb.cptr, pb.pptr, pb.pidx, n, h->E.as<int32_t>(),
+                                   h->nk.as<int32_t>(), st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));  // max_col_nnz is on the host now
+    BucketRule rule{};
+    rule.single_bucket = prm->batched ? -1 : 2;
+    rule.allow_warp = adaptive ? 0 : 1;
+    rule.warp_emax = 64;
+    rule.warp_nmax = 16;
+    rule.smem_w_bytes = 96 * 1024;
+    rule.elem_bytes = elem;
+    rule.grow_n = grow_n;
+    rule.grow_e = adaptive ? grow_n * max_col_nnz : 0;
+    CUDA_TRY(h, cudaMemsetAsync(dcnt, 0, sizeof(int32_t) * 16, st));
+    CUDA_TRY(h, mspai::launch_bucket(h->E.as<int32_t>(), h->nk.as<int32_t>(), n, rule, dcnt,
+                                     dcnt + 4, dcnt + 8, h->lists.as<int32_t>(), st));
+    int32_t hc[16];
+    CUDA_TRY(h, cudaMemcpyAsync(hc, dcnt, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+
+    // ---- bucket kernels
+    for (int b = 0; b < kBuckets; b++)
+        h->stats.bucket_columns[b] = hc[b];
+    h->stats.bucket_columns[3] = 0;
+    for (int b = 0; b < kBuckets; b++) {
+        const int count = hc[b];
+        h->stats.kernel_ms[b] = 0.0;
+        if (count == 0)
+            continue;
+        Caps cap{};
+        cap.emax = std::max(1, hc[4 + b]);
+        cap.nmax = std::max(1, hc[8 + b]);
+        cap.lsort = mspai::next_pow2(cap.emax);
+        cap.mwmax = cap.emax / 2 + cap.nmax;
+        cap.cmax = adaptive ? (cap.emax + 1) * std::max(1, max_row_nnz) : 0;
+        cap.lcand = adaptive ? mspai::next_pow2(cap.cmax) : 0;
+        if (static_cast<int64_t>(cap.emax) >= mspai::kMaxEntries)
+            return set_err(h, MSPAI_ERR_CAPACITY, "a column touches %d entries of C (max %d)",
+                           cap.emax, mspai::kMaxEntries - 1);
+        int32_t* list = h->lists.as<int32_t>() + static_cast<size_t>(b) * n;
+        int32_t* counter = dcnt + 12 + b;
+        CUDA_TRY(h, cudaMemsetAsync(counter, 0, sizeof(int32_t), st));
+        CUDA_TRY(h, cudaEventRecord(h->evb[2 * b], st));
+        int grid = 0;
+        bool use_warp = (b == 0);
+        if (use_warp &&
+            mspai::warp_slot_bytes(cap, elem) * (mspai::kWarpKernelThreads / 32) > 200 * 1024)
+            use_warp = false;
+        if (use_warp) {
+            CUDA_TRY(h, mspai::launch_warp_solve(elem, pb, cap, out, list, count, counter, st,
+                                                 &grid));
+        }
+        else {
+            const bool wsm = (b == 1) && mspai::w_bytes(cap, elem) <= 200 * 1024;
+            const size_t need = mspai::cta_scratch_needed(elem, wsm, cap, count);
+            CUDA_TRY(h, h->scratch.ensure(need));
+            CUDA_TRY(h, mspai::launch_cta_solve(elem, wsm, pb, cap, out, list, count, counter,
+                                                h->scratch.as<char>(), h->scratch.bytes, st,
+                                                &grid));
+        }
+        CUDA_TRY(h, cudaEventRecord(h->evb[2 * b + 1], st));
+    }
+
+    // ---- assemble M
+    if (adaptive) {
+        CUDA_TRY(h, h->mptr.ensure(sizeof(int64_t) * (n + 1)));
+        CUDA_TRY(h, mspai::launch_scan_lengths(out.olen, n, h->mptr.as<int64_t>(),
+                                               h->scan_tmp.as<int64_t>(), st));
+        int64_t nnz = 0;
+        CUDA_TRY(h, cudaMemcpyAsync(&nnz, h->mptr.as<int64_t>() + n, sizeof(int64_t),
+                                    cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(h, cudaStreamSynchronize(st));
+        CUDA_TRY(h, h->midx.ensure(sizeof(int32_t) * std::max<int64_t>(nnz, 1)));
+        CUDA_TRY(h, h->mval.ensure(sizeof(double) * std::max<int64_t>(nnz, 1)));
+        CUDA_TRY(h, mspai::launch_compact(out.optr, out.oidx, out.oval, h->mptr.as<int64_t>(),
+                                          h->midx.as<int32_t>(), h->mval.as<double>(), n, st));
+        h->nnz_m = nnz;
+        h->res_ptr = h->mptr.as<int64_t>();
+        h->res_idx = h->midx.as<int32_t>();
+        h->res_val = h->mval.as<double>();
+    }
+    else {
+        h->nnz_m = P->nnz;
+        h->res_ptr = pb.pptr;
+        h->res_idx = pb.pidx;
+        h->res_val = out.oval;
+        if (P->mem == MSPAI_MEM_HOST) {
+            // keep the structure alive in the handle's buffers (already staged)
+        }
+        else {
+            // borrowed device pattern: copy so the result outlives the call
+            CUDA_TRY(h, h->mptr.ensure(sizeof(int64_t) * (n + 1)));
+            CUDA_TRY(h, h->midx.ensure(sizeof(int32_t) * std::max<int64_t>(P->nnz, 1)));
+            CUDA_TRY(h, cudaMemcpyAsync(h->mptr.p, pb.pptr, sizeof(int64_t) * (n + 1),
+                                        cudaMemcpyDeviceToDevice, st));
+            if (P->nnz > 0)
+                CUDA_TRY(h, cudaMemcpyAsync(h->midx.p, pb.pidx, sizeof(int32_t) * P->nnz,
+                                            cudaMemcpyDeviceToDevice, st));
+            h->res_ptr = h->mptr.as<int64_t>();
+            h->res_idx = h->midx.as<int32_t>();
+        }
+    }
+    CUDA_TRY(h, cudaEventRecord(h->ev1, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    CUDA_TRY(h, cudaGetLastError());
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->stats.setup_ms = ms;
+    for (int b = 0; b < kBuckets; b++) {
+        if (hc[b] > 0) {
+            float kms = 0.f;
+            cudaEventElapsedTime(&kms, h->evb[2 * b], h->evb[2 * b + 1]);
+            h->stats.kernel_ms[b] = kms;
+        }
+    }
+    h->stats.columns = n;
+    h->stats.nnz_m = h->nnz_m;
+    h->last_params = *prm;
+    h->have_result = true;
+    return MSPAI_OK;
+}
+
+int mspai_result_nnz(mspai_handle* h, int64_t* nnz)
+{
+    if (!h || !h->have_result)
+        return h ? set_err(h, MSPAI_ERR_STATE, "no setup result") : MSPAI_ERR_STATE;
+    *nnz = h->nnz_m;
+    return MSPAI_OK;
+}
+
+int mspai_result_copy(mspai_handle* h, int64_t* colptr, int32_t* rowidx, double* values,
+                      int32_t mem)
+{
+    if (!h || !h->have_result)
+        return h ? set_err(h, MSPAI_ERR_STATE, "no setup result") : MSPAI_ERR_STATE;
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    const cudaMemcpyKind k = mem == MSPAI_MEM_DEVICE ? cudaMemcpyDeviceToDevice
+                                                     : cudaMemcpyDeviceToHost;
+    cudaStream_t st = h->stream;
+    if (colptr)
+        CUDA_TRY(h, cudaMemcpyAsync(colptr, h->res_ptr, sizeof(int64_t) * (h->n + 1), k, st));
+    if (rowidx && h->nnz_m > 0)
+        CUDA_TRY(h, cudaMemcpyAsync(rowidx, h->res_idx, sizeof(int32_t) * h->nnz_m, k, st));
+    if (values && h->nnz_m > 0)
+        CUDA_TRY(h, cudaMemcpyAsync(values, h->res_val, sizeof(double) * h->nnz_m, k, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    return MSPAI_OK;
+}
+
+int mspai_column_info(mspai_handle* h, double* resnorm, int32_t* steps, int32_t* status)
+{
+    if (!h || !h->have_result)
+        return h ? set_err(h, MSPAI_ERR_STATE, "no setup result") : MSPAI_ERR_STATE;
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    if (resnorm)
+        CUDA_TRY(h, cudaMemcpyAsync(resnorm, h->res.p, sizeof(double) * h->n,
+                                    cudaMemcpyDeviceToHost, st));
+    if (steps)
+        CUDA_TRY(h, cudaMemcpyAsync(steps, h->steps.p, sizeof(int32_t) * h->n,
+                                    cudaMemcpyDeviceToHost, st));
+    if (status)
+        CUDA_TRY(h, cudaMemcpyAsync(status, h->status.p, sizeof(int32_t) * h->n,
+                                    cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    return MSPAI_OK;
+}
+
+int mspai_get_stats(mspai_handle* h, mspai_stats* s)
+{
+    if (!h || !h->have_result)
+        return h ? set_err(h, MSPAI_ERR_STATE, "no setup result") : MSPAI_ERR_STATE;
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    std::vector<double> work(3 * static_cast<size_t>(h->n));
+    std::vector<int32_t> steps(h->n), status(h->n);
+    if (h->n > 0) {
+        CUDA_TRY(h, cudaMemcpyAsync(work.data(), h->work.p, sizeof(double) * work.size(),
+                                    cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(h, cudaMemcpyAsync(steps.data(), h->steps.p, sizeof(int32_t) * h->n,
+                                    cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(h, cudaMemcpyAsync(status.data(), h->status.p, sizeof(int32_t) * h->n,
+                                    cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    }
+    double fl = 0.0, fld = 0.0, by = 0.0;
+    int64_t solves = 0, sing = 0, capc = 0;
+    for (int c = 0; c < h->n; c++) {
+        fl += work[3 * c];
+        fld += work[3 * c + 1];
+        by += work[3 * c + 2];
+        solves += steps[c];
+        sing += status[c] == MSPAI_COL_SINGULAR;
+        capc += status[c] == MSPAI_COL_CAPACITY;
+    }
+    h->stats.flops = fl;
+    h->stats.flops_dense = fld;
+    h->stats.gather_bytes = by;
+    h->stats.ls_solves = solves;
+    h->stats.singular_columns = sing;
+    h->stats.capacity_columns = capc;
+    *s = h->stats;
+    return MSPAI_OK;
+}
+
+}  // extern "C"
+
+extern "C" int mspai_adjoint(mspai_handle* h, const mspai_csc* C, const mspai_csc* B,
+                             const double* gbar_values, double* dC_values, double* dB_values,
+                             double* loss, int32_t mem)
+{
+    if (!h || !h->have_result)
+        return h ? set_err(h, MSPAI_ERR_STATE, "no setup result") : MSPAI_ERR_STATE;
+    if (!h->fixed_pattern)
+        return set_err(h, MSPAI_ERR_STATE,
+                       "the adjoint needs a fixed-pattern setup (ns = 0): the pattern update "
+                       "is not differentiable");
+    if (!C || !dC_values)
+        return set_err(h, MSPAI_ERR_PARAM, "C and dC are required");
+    if (C->ncols != h->n)
+        return set_err(h, MSPAI_ERR_INPUT, "C does not match the last setup");
+    if (B && (B->ncols != h->n || B->nrows != C->nrows))
+        return set_err(h, MSPAI_ERR_INPUT, "B does not match C");
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    const int n = h->n;
+    Problem pb{};
+    pb.n = n;
+    pb.nrows = C->nrows;
+    CUDA_TRY(h, stage(h->cptr, C->colptr, n + 1, C->mem, st, &pb.cptr));
+    CUDA_TRY(h, stage(h->cidx, C->rowidx, C->nnz, C->mem, st, &pb.cidx));
+    CUDA_TRY(h, stage(h->cval, C->values, C->nnz, C->mem, st, &pb.cval));
+    if (B) {
+        CUDA_TRY(h, stage(h->bptr, B->colptr, n + 1, B->mem, st, &pb.bptr));
+        CUDA_TRY(h, stage(h->bidx, B->rowidx, B->nnz, B->mem, st, &pb.bidx));
+        CUDA_TRY(h, stage(h->bval, B->values, B->nnz, B->mem, st, &pb.bval));
+    }
+    pb.pptr = h->res_ptr;
+    pb.pidx = h->res_idx;
+    mspai::AdjointIO io{};
+    io.mptr = h->res_ptr;
+    DevBuf gbuf, dcbuf, dbbuf, lossbuf, cnt;
+    if (gbar_values) {
+        const double* gp = nullptr;
+        CUDA_TRY(h, stage(gbuf, gbar_values, static_cast<size_t>(h->nnz_m), mem, st, &gp));
+        io.gbar = gp;
+    }
+    if (mem == MSPAI_MEM_DEVICE) {
+        io.dC = dC_values;
+        io.dB = B ? dB_values : nullptr;
+    }
+    else {
+        CUDA_TRY(h, dcbuf.ensure(sizeof(double) * std::max<int64_t>(C->nnz, 1)));
+        io.dC = dcbuf.as<double>();
+        if (B && dB_values) {
+            CUDA_TRY(h, dbbuf.ensure(sizeof(double) * std::max<int64_t>(B->nnz, 1)));
+            io.dB = dbbuf.as<double>();
+        }
+    }
+    CUDA_TRY(h, cudaMemsetAsync(io.dC, 0, sizeof(double) * C->nnz, st));
+    CUDA_TRY(h, lossbuf.ensure(sizeof(double) * std::max(n, 1)));
+    io.loss = lossbuf.as<double>();
+    CUDA_TRY(h, cudaMemsetAsync(io.loss, 0, sizeof(double) * std::max(n, 1), st));
+    // sizes
+    CUDA_TRY(h, cnt.ensure(64 * sizeof(int32_t)));
+    int32_t* dcnt = cnt.as<int32_t>();
+    CUDA_TRY(h, cudaMemsetAsync(dcnt, 0, 64 * sizeof(int32_t), st));
+    CUDA_TRY(h, h->E.ensure(sizeof(int32_t) * std::max(n, 1)));
+    CUDA_TRY(h, h->nk.ensure(sizeof(int32_t) * std::max(n, 1)));
+    CUDA_TRY(h, h->lists.ensure(sizeof(int32_t) * 3 * static_cast<size_t>(std::max(n, 1))));
+    CUDA_TRY(h, mspai::launch_plan(pb.cptr, pb.pptr, pb.pidx, n, h->E.as<int32_t>(),
+                                   h->nk.as<int32_t>(), st));
+    BucketRule rule{};
+    rule.single_bucket = 0;
+    rule.elem_bytes = 8;
+    CUDA_TRY(h, mspai::launch_bucket(h->E.as<int32_t>(), h->nk.as<int32_t>(), n, rule, dcnt,
+                                     dcnt + 4, dcnt + 8, h->lists.as<int32_t>(), st));
+    int32_t hc[16];
+    CUDA_TRY(h, cudaMemcpyAsync(hc, dcnt, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    Caps cap{};
+    cap.emax = std::max(1, hc[4]);
+    cap.nmax = std::max(1, hc[8]);
+    cap.lsort = mspai::next_pow2(cap.emax);
+    cap.mwmax = cap.emax / 2 + cap.nmax;
+    cap.cmax = cap.emax;  // q = C lambda is kept in the rho[] area
+    cap.lcand = 0;
+    const bool warp = cap.emax <= 64 && cap.nmax <= 16;
+    const size_t need = mspai::adjoint_scratch_bytes(cap, n, warp);
+    CUDA_TRY(h, h->scratch.ensure(need));
+    CUDA_TRY(h, cudaMemsetAsync(dcnt + 20, 0, sizeof(int32_t), st));
+    CUDA_TRY(h, mspai::launch_adjoint(pb, cap, io, n, warp, h->scratch.as<char>(),
+                                      h->scratch.bytes, dcnt + 20, st));
+    std::vector<double> hl(n);
+    if (n > 0)
+        CUDA_TRY(h, cudaMemcpyAsync(hl.data(), io.loss, sizeof(double) * n,
+                                    cudaMemcpyDeviceToHost, st));
+    if (mem == MSPAI_MEM_HOST) {
+        CUDA_TRY(h, cudaMemcpyAsync(dC_values, io.dC, sizeof(double) * C->nnz,
+                                    cudaMemcpyDeviceToHost, st));
+        if (io.dB)
+            CUDA_TRY(h, cudaMemcpyAsync(dB_values, io.dB, sizeof(double) * B->nnz,
+                                        cudaMemcpyDeviceToHost, st));
+    }
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    CUDA_TRY(h, cudaGetLastError());
+    if (loss) {
+        double s = 0.0;
+        for (double v : hl)
+            s += v;
+        *loss = s;
+    }
+    gbuf.release();
+    dcbuf.release();
+    dbbuf.release();
+    lossbuf.release();
+    cnt.release();
+    return MSPAI_OK;
+}

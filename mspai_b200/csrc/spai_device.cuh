@@ -1,0 +1,192 @@
+// Device building blocks of the batched MSPAI column solver (sm_100a).
+//
+// A "group" is the set of threads that cooperates on one column problem:
+// either one warp (WarpGroup, tiny problems, everything in shared memory) or
+// one CTA (CtaGroup<NT>, larger problems, workspace in global scratch that
+// stays resident in L2).  All routines below are written against the group
+// interface, so the same per-column algorithm runs at both granularities.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mspai {
+
+constexpr int kEntryBits = 24;  // sort key = (row << 24) | entry index
+constexpr uint64_t kEntryMask = (uint64_t(1) << kEntryBits) - 1;
+constexpr int kMaxEntries = 1 << kEntryBits;
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_sum(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ int warp_sum(int v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Shared scratch a group needs for reductions and broadcasts.
+struct GroupScratch {
+    double red[32];
+    double d[4];
+    int i[8];
+};
+
+struct WarpGroup {
+    GroupScratch* sc;
+    static constexpr int kSize = 32;
+    static constexpr int kWarps = 1;
+    __device__ __forceinline__ int rank() const { return threadIdx.x & 31; }
+    __device__ __forceinline__ int warp() const { return 0; }
+    __device__ __forceinline__ int lane() const { return threadIdx.x & 31; }
+    __device__ __forceinline__ void sync() const { __syncwarp(); }
+    template <class T>
+    __device__ __forceinline__ T sum(T v) const
+    {
+        return warp_sum(v);
+    }
+    __device__ __forceinline__ int bcast(int v) const { return __shfl_sync(0xffffffffu, v, 0); }
+};
+
+template <int NT>
+struct CtaGroup {
+    GroupScratch* sc;
+    static constexpr int kSize = NT;
+    static constexpr int kWarps = NT / 32;
+    __device__ __forceinline__ int rank() const { return threadIdx.x; }
+    __device__ __forceinline__ int warp() const { return threadIdx.x >> 5; }
+    __device__ __forceinline__ int lane() const { return threadIdx.x & 31; }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+    template <class T>
+    __device__ __forceinline__ T sum(T v) const
+    {
+        v = warp_sum(v);
+        if (lane() == 0)
+            sc->red[warp()] = static_cast<double>(v);
+        __syncthreads();
+        double t = 0.0;
+        if (threadIdx.x < 32) {
+            t = threadIdx.x < kWarps ? sc->red[threadIdx.x] : 0.0;
+            t = warp_sum(t);
+            if (threadIdx.x == 0)
+                sc->d[3] = t;
+        }
+        __syncthreads();
+        t = sc->d[3];
+        __syncthreads();
+        return static_cast<T>(t);
+    }
+    __device__ __forceinline__ int bcast(int v) const
+    {
+        if (threadIdx.x == 0)
+            sc->i[7] = v;
+        __syncthreads();
+        int r = sc->i[7];
+        __syncthreads();
+        return r;
+    }
+};
+
+// Exclusive prefix sum of a[0..len) in place; returns the total.  Each thread
+// scans a contiguous chunk; the thread totals are scanned with warp shuffles.
+template <class G>
+__device__ int group_exclusive_scan(const G& g, int* a, int len)
+{
+    const int chunk = (len + G::kSize - 1) / G::kSize;
+    const int lo = min(g.rank() * chunk, len);
+    const int hi = min(lo + chunk, len);
+    int s = 0;
+    for (int i = lo; i < hi; i++)
+        s += a[i];
+    // inclusive warp scan of the thread totals
+    int v = s;
+    const int lane = g.lane();
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o)
+            v += t;
+    }
+    int* part = reinterpret_cast<int*>(g.sc->red);
+    if constexpr (G::kWarps > 1) {
+        if (lane == 31)
+            part[g.warp()] = v;
+        g.sync();
+        if (g.rank() == 0) {
+            int run = 0;
+            for (int w = 0; w < G::kWarps; w++) {
+                const int t = part[w];
+                part[w] = run;
+                run += t;
+            }
+            g.sc->i[6] = run;
+        }
+        g.sync();
+        int run = part[g.warp()] + v - s;
+        for (int i = lo; i < hi; i++) {
+            const int t = a[i];
+            a[i] = run;
+            run += t;
+        }
+        const int total = g.sc->i[6];
+        g.sync();
+        return total;
+    }
+    else {
+        const int total = __shfl_sync(0xffffffffu, v, 31);
+        int run = v - s;
+        for (int i = lo; i < hi; i++) {
+            const int t = a[i];
+            a[i] = run;
+            run += t;
+        }
+        __syncwarp();
+        return total;
+    }
+}
+
+// Bitonic sort of keys[0..L), L a power of two (pad with the maximum key).
+template <class G, class K>
+__device__ void group_bitonic_sort(const G& g, K* keys, int L)
+{
+    for (int k = 2; k <= L; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = g.rank(); i < L; i += G::kSize) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const K a = keys[i];
+                    const K b = keys[ixj];
+                    const bool up = (i & k) == 0;
+                    if ((a > b) == up) {
+                        keys[i] = b;
+                        keys[ixj] = a;
+                    }
+                }
+            }
+            g.sync();
+        }
+    }
+}
+
+__host__ __device__ inline int next_pow2(int v)
+{
+    int p = 1;
+    while (p < v)
+        p <<= 1;
+    return p;
+}
+
+}  // namespace mspai

