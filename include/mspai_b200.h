@@ -119,6 +119,8 @@ typedef struct {
     double gather_bytes;      /* algorithmic gather/assembly bytes           */
     double setup_ms;          /* device time of the last setup (CUDA events) */
     double kernel_ms[4];      /* device time per bucket kernel               */
+    int64_t kernel_launches;  /* kernels this library launched in the setup  */
+    double bucket_flops[4];   /* algorithmic (folded) flops per bucket kernel */
 } mspai_stats;
 
 typedef struct mspai_handle mspai_handle;
@@ -187,6 +189,14 @@ const char* mspai_last_error(mspai_handle* h);
 
 /* Releases the handle and its device memory. */
 void mspai_free(mspai_handle* h);
+
+/*
+ * Measures the FP32 (fp64 == 0) or FP64 (fp64 == 1) fused-multiply-add
+ * throughput of CUDA device `device` with independent register-resident FMA
+ * chains on every SM: the CUDA-core roofline denominator of the
+ * least-squares kernels.  Writes GFLOP/s (2 flops per FMA) to *gflops.
+ */
+int mspai_measure_fma_peak(int32_t device, int32_t fp64, double* gflops);
 
 /* Library version string. */
 const char* mspai_version(void);

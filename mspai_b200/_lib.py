@@ -44,7 +44,8 @@ class mspai_stats(ctypes.Structure):
                 ("capacity_columns", ctypes.c_int64), ("bucket_columns", ctypes.c_int64 * 4),
                 ("flops", ctypes.c_double), ("flops_dense", ctypes.c_double),
                 ("gather_bytes", ctypes.c_double), ("setup_ms", ctypes.c_double),
-                ("kernel_ms", ctypes.c_double * 4)]
+                ("kernel_ms", ctypes.c_double * 4), ("kernel_launches", ctypes.c_int64),
+                ("bucket_flops", ctypes.c_double * 4)]
 
 
 class mspai_matrix(ctypes.Structure):
@@ -61,6 +62,7 @@ EXPORTED = [
     "mspai_adjoint", "mspai_last_error", "mspai_free", "mspai_version",
     "mspai_matrix_view", "mspai_matrix_free", "mspai_mm_read", "mspai_mm_write",
     "mspai_probing_assemble", "mspai_pattern_generate", "mspai_row_structure",
+    "mspai_measure_fma_peak",
 ]
 
 _lib = None
@@ -100,6 +102,9 @@ def load() -> ctypes.CDLL:
     lib.mspai_last_error.restype = ctypes.c_char_p
     lib.mspai_free.argtypes = [V]
     lib.mspai_free.restype = None
+    lib.mspai_measure_fma_peak.argtypes = [ctypes.c_int32, ctypes.c_int32,
+                                           ctypes.POINTER(ctypes.c_double)]
+    lib.mspai_measure_fma_peak.restype = I
     lib.mspai_version.argtypes = []
     lib.mspai_version.restype = ctypes.c_char_p
     lib.mspai_mm_read.argtypes = [ctypes.c_char_p, P(mspai_matrix), ctypes.c_char_p,

@@ -68,8 +68,9 @@ class Options:
 
 
 class DeviceCSC:
-    """A CSC matrix resident on the GPU (torch tensors: int64 colptr, int32
-    rowidx, float64 values or None for a pattern)."""
+    """A CSC matrix held in torch tensors (int64 colptr, int32 rowidx, float64
+    values or None for a pattern): on the GPU (already resident in HBM) or in
+    pinned host memory (copied by the library inside the setup)."""
 
     def __init__(self, nrows: int, ncols: int, colptr, rowidx, values=None):
         self.nrows, self.ncols = int(nrows), int(ncols)
@@ -79,14 +80,29 @@ class DeviceCSC:
     def nnz(self) -> int:
         return int(self.rowidx.numel())
 
+    @property
+    def on_device(self) -> bool:
+        return bool(self.colptr.is_cuda)
+
     @staticmethod
-    def from_scipy(M: sp.spmatrix, device="cuda", pattern: bool = False) -> "DeviceCSC":
+    def from_scipy(M: sp.spmatrix, device="cuda", pattern: bool = False,
+                   pin: bool = False) -> "DeviceCSC":
         import torch
+
+        def conv(a, dt):
+            t = torch.from_numpy(np.ascontiguousarray(a, dtype=dt))
+            if str(device) == "cpu":
+                return t.pin_memory() if pin else t
+            return t.to(device)
         M = _canon(M)
-        cp = torch.from_numpy(np.asarray(M.indptr, dtype=np.int64)).to(device)
-        ri = torch.from_numpy(np.asarray(M.indices, dtype=np.int32)).to(device)
-        v = None if pattern else torch.from_numpy(np.asarray(M.data, dtype=np.float64)).to(device)
+        cp = conv(M.indptr, np.int64)
+        ri = conv(M.indices, np.int32)
+        v = None if pattern else conv(M.data, np.float64)
         return DeviceCSC(M.shape[0], M.shape[1], cp, ri, v)
+
+    def nbytes(self) -> int:
+        b = self.colptr.numel() * 8 + self.rowidx.numel() * 4
+        return b + (self.values.numel() * 8 if self.values is not None else 0)
 
 
 def _canon(M: sp.spmatrix) -> sp.csc_matrix:
@@ -105,7 +121,7 @@ class _Staged:
             self.keep = (M.colptr, M.rowidx, M.values)
             self.c = mspai_csc(M.nrows, M.ncols, M.nnz, M.colptr.data_ptr(), M.rowidx.data_ptr(),
                                None if (pattern or M.values is None) else M.values.data_ptr(),
-                               MEM_DEVICE)
+                               MEM_DEVICE if M.on_device else MEM_HOST)
             return
         M = _canon(M)
         cp = np.ascontiguousarray(M.indptr, dtype=np.int64)
@@ -206,6 +222,7 @@ class Handle:
             "bucket_columns": list(s.bucket_columns)[:3], "flops": s.flops,
             "flops_dense": s.flops_dense, "gather_bytes": s.gather_bytes,
             "setup_ms": s.setup_ms, "kernel_ms": list(s.kernel_ms)[:3],
+            "kernel_launches": s.kernel_launches, "bucket_flops": list(s.bucket_flops)[:3],
         }
 
     def adjoint(self, C: MatrixLike, B: Optional[MatrixLike] = None,
@@ -228,6 +245,15 @@ class Handle:
                                      ctypes.byref(loss), MEM_HOST)
         self._check(rc)
         return dC[:sc.c.nnz], (dB[:sb.c.nnz] if dB is not None else None), float(loss.value)
+
+
+def measure_fma_peak(device: int = 0, fp64: bool = False) -> float:
+    """FP32 / FP64 CUDA-core FMA throughput in GFLOP/s (mspai_measure_fma_peak)."""
+    v = ctypes.c_double()
+    rc = _lib.load().mspai_measure_fma_peak(int(device), 1 if fp64 else 0, ctypes.byref(v))
+    if rc != _lib.MSPAI_OK:
+        raise MspaiError(rc, "FMA peak probe failed")
+    return float(v.value)
 
 
 def assemble_probing(A: sp.spmatrix, Ce: Optional[sp.spmatrix], Be: Optional[sp.spmatrix],

@@ -90,6 +90,7 @@ struct mspai_handle {
     const double* res_val = nullptr;
     mspai_stats stats{};
     mspai_params last_params{};
+    int64_t launches = 0;
 };
 
 static int set_err(mspai_handle* h, int code, const char* fmt, ...)
@@ -362,11 +363,13 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     const int elem = mixed ? 4 : 8;
 
     // ---- time the device part of the setup
+    h->launches = 0;
     CUDA_TRY(h, cudaEventRecord(h->ev0, st));
 
     // max column nnz of C (growth bound of the entry count)
     CUDA_TRY(h, h->counters.ensure(64 * sizeof(int32_t)));
     int32_t* dcnt = h->counters.as<int32_t>();
+    h->launches++;
     CUDA_TRY(h, mspai::launch_max_len(pb.cptr, n, dcnt + 16, st));
     CUDA_TRY(h, cudaMemcpyAsync(&max_col_nnz, dcnt + 16, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
 
@@ -384,7 +387,9 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     if (adaptive) {
         CUDA_TRY(h, h->cap_len.ensure(sizeof(int32_t) * std::max(n, 1)));
         CUDA_TRY(h, h->cap_ptr.ensure(sizeof(int64_t) * (n + 1)));
-        CUDA_TRY(h, mspai::launch_capacity_len(pb.pptr, n, grow_n, h->cap_len.as<int32_t>(), st));
+        h->launches++;
+    CUDA_TRY(h, mspai::launch_capacity_len(pb.pptr, n, grow_n, h->cap_len.as<int32_t>(), st));
+        h->launches += 4;
         CUDA_TRY(h, mspai::launch_scan_lengths(h->cap_len.as<int32_t>(), n, h->cap_ptr.as<int64_t>(),
                                                h->scan_tmp.as<int64_t>(), st));
         cap_total = P->nnz + static_cast<int64_t>(grow_n) * n;
@@ -410,6 +415,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     CUDA_TRY(h, h->E.ensure(sizeof(int32_t) * std::max(n, 1)));
     CUDA_TRY(h, h->nk.ensure(sizeof(int32_t) * std::max(n, 1)));
     CUDA_TRY(h, h->lists.ensure(sizeof(int32_t) * static_cast<size_t>(kBuckets) * std::max(n, 1)));
+    h->launches++;
     CUDA_TRY(h, mspai::launch_plan(pb.cptr, pb.pptr, pb.pidx, n, h->E.as<int32_t>(),
                                    h->nk.as<int32_t>(), st));
     CUDA_TRY(h, cudaStreamSynchronize(st));  // max_col_nnz is on the host now
@@ -423,6 +429,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     rule.grow_n = grow_n;
     rule.grow_e = adaptive ? grow_n * max_col_nnz : 0;
     CUDA_TRY(h, cudaMemsetAsync(dcnt, 0, sizeof(int32_t) * 16, st));
+    h->launches++;
     CUDA_TRY(h, mspai::launch_bucket(h->E.as<int32_t>(), h->nk.as<int32_t>(), n, rule, dcnt,
                                      dcnt + 4, dcnt + 8, h->lists.as<int32_t>(), st));
     int32_t hc[16];
@@ -458,6 +465,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
             mspai::warp_slot_bytes(cap, elem) * (mspai::kWarpKernelThreads / 32) > 200 * 1024)
             use_warp = false;
         if (use_warp) {
+            h->launches++;
             CUDA_TRY(h, mspai::launch_warp_solve(elem, pb, cap, out, list, count, counter, st,
                                                  &grid));
         }
@@ -465,6 +473,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
             const bool wsm = (b == 1) && mspai::w_bytes(cap, elem) <= 200 * 1024;
             const size_t need = mspai::cta_scratch_needed(elem, wsm, cap, count);
             CUDA_TRY(h, h->scratch.ensure(need));
+            h->launches++;
             CUDA_TRY(h, mspai::launch_cta_solve(elem, wsm, pb, cap, out, list, count, counter,
                                                 h->scratch.as<char>(), h->scratch.bytes, st,
                                                 &grid));
@@ -475,6 +484,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     // ---- assemble M
     if (adaptive) {
         CUDA_TRY(h, h->mptr.ensure(sizeof(int64_t) * (n + 1)));
+        h->launches += 4;
         CUDA_TRY(h, mspai::launch_scan_lengths(out.olen, n, h->mptr.as<int64_t>(),
                                                h->scan_tmp.as<int64_t>(), st));
         int64_t nnz = 0;
@@ -483,7 +493,8 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
         CUDA_TRY(h, cudaStreamSynchronize(st));
         CUDA_TRY(h, h->midx.ensure(sizeof(int32_t) * std::max<int64_t>(nnz, 1)));
         CUDA_TRY(h, h->mval.ensure(sizeof(double) * std::max<int64_t>(nnz, 1)));
-        CUDA_TRY(h, mspai::launch_compact(out.optr, out.oidx, out.oval, h->mptr.as<int64_t>(),
+        h->launches++;
+    CUDA_TRY(h, mspai::launch_compact(out.optr, out.oidx, out.oval, h->mptr.as<int64_t>(),
                                           h->midx.as<int32_t>(), h->mval.as<double>(), n, st));
         h->nnz_m = nnz;
         h->res_ptr = h->mptr.as<int64_t>();
@@ -526,6 +537,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     }
     h->stats.columns = n;
     h->stats.nnz_m = h->nnz_m;
+    h->stats.kernel_launches = h->launches;
     h->last_params = *prm;
     h->have_result = true;
     return MSPAI_OK;
@@ -595,6 +607,17 @@ int mspai_get_stats(mspai_handle* h, mspai_stats* s)
     }
     double fl = 0.0, fld = 0.0, by = 0.0;
     int64_t solves = 0, sing = 0, capc = 0;
+    // algorithmic flops per bucket kernel (columns listed per bucket)
+    for (int b = 0; b < 4; b++)
+        h->stats.bucket_flops[b] = 0.0;
+    if (h->n > 0 && h->lists.p) {
+        std::vector<int32_t> lists(static_cast<size_t>(kBuckets) * h->n);
+        CUDA_TRY(h, cudaMemcpy(lists.data(), h->lists.p, sizeof(int32_t) * lists.size(),
+                               cudaMemcpyDeviceToHost));
+        for (int b = 0; b < kBuckets; b++)
+            for (int64_t t = 0; t < h->stats.bucket_columns[b]; t++)
+                h->stats.bucket_flops[b] += work[3 * static_cast<size_t>(lists[b * static_cast<size_t>(h->n) + t])];
+    }
     for (int c = 0; c < h->n; c++) {
         fl += work[3 * c];
         fld += work[3 * c + 1];
@@ -678,11 +701,13 @@ extern "C" int mspai_adjoint(mspai_handle* h, const mspai_csc* C, const mspai_cs
     CUDA_TRY(h, h->E.ensure(sizeof(int32_t) * std::max(n, 1)));
     CUDA_TRY(h, h->nk.ensure(sizeof(int32_t) * std::max(n, 1)));
     CUDA_TRY(h, h->lists.ensure(sizeof(int32_t) * 3 * static_cast<size_t>(std::max(n, 1))));
+    h->launches++;
     CUDA_TRY(h, mspai::launch_plan(pb.cptr, pb.pptr, pb.pidx, n, h->E.as<int32_t>(),
                                    h->nk.as<int32_t>(), st));
     BucketRule rule{};
     rule.single_bucket = 0;
     rule.elem_bytes = 8;
+    h->launches++;
     CUDA_TRY(h, mspai::launch_bucket(h->E.as<int32_t>(), h->nk.as<int32_t>(), n, rule, dcnt,
                                      dcnt + 4, dcnt + 8, h->lists.as<int32_t>(), st));
     int32_t hc[16];

@@ -1,6 +1,11 @@
 """Adjoint of the fixed-pattern setup against central finite differences
-(step 1e-6, relative agreement 1e-6), a closed form, and a dense FP64 QR
-reference gradient."""
+(step 1e-6 relative to the parameter, agreement 1e-6 relative), a closed form,
+and a dense FP64 QR reference loss.
+
+Relative agreement is measured against max(|g|, 1e-3 * L / rho) for the
+weight rho: near rho = 100 the probing rows are almost satisfied and dL/drho
+falls to ~1e-7 while the loss is O(1), so the finite-difference quotient's own
+rounding (~1e-16 L / step) is the floor, not the adjoint."""
 import numpy as np
 import pytest
 import scipy.sparse as sp
@@ -69,7 +74,7 @@ def test_drho_finite_difference_and_closed_form(h, kinds, rho):
     Lp = loss_and_grad(h, w.A, w.Ce, w.Be, rho + hstep, w.P)[5]
     Lm = loss_and_grad(h, w.A, w.Ce, w.Be, rho - hstep, w.P)[5]
     fd = (Lp - Lm) / (2 * hstep)
-    assert abs(fd - g) <= FD_TOL * max(abs(g), 1e-12)
+    assert abs(fd - g) <= FD_TOL * max(abs(g), 1e-3 * L / rho)
 
 
 def test_dA_finite_difference(h):
@@ -118,7 +123,7 @@ def test_gbar_term_finite_difference(h):
         Cp, Bp, Mp, *_ = loss_and_grad(h, w.A, w.Ce, w.Be, rho + sgn * hstep, w.P)
         vals.append(np.sum(column_residuals(Cp, Mp, Bp) ** 2) + np.dot(gbar, Mp.data))
     fd = (vals[0] - vals[1]) / (2 * hstep)
-    assert abs(fd - g) <= FD_TOL * max(abs(g), 1e-12)
+    assert abs(fd - g) <= FD_TOL * max(abs(g), 1e-3 * abs(L) / rho)
 
 
 def test_loss_matches_dense_qr_reference(h):
