@@ -1,0 +1,407 @@
+#!/usr/bin/env python
+"""Setup throughput of the MSPAI preconditioner on B200.
+
+Metric: setup columns/s on 1 B200, batched mixed (FP32 Householder QR + FP64
+refinement, size-bucketed kernels) vs the plain per-column FP64 GPU path, at
+equal ||AM - I||_F.
+
+Workload (one "step"): the full fixed-pattern setup of the ragged 1M-column
+matrix -- A n = 1,000,000, U{4..32} random off-diagonal rows per column,
+values N(0,1), diagonal 1.5 * sum |off|; P = pattern(A^2) with entries below
+1e-3 of the column max dropped (|J_k| 18..293, mean 134); seeded synthetic
+data (no public matrix collection is named).  Every rank solves its own
+1M-column block (seed + rank): weak scaling, no data-path collective.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line on rank 0.  `value` is measured with the inputs resident
+in HBM; `e2e` is the same metric through the public API from pinned host
+buffers, host<->device copies inside the timed region.  The reference arm
+(--impl reference) times the reference's own CPU column loop (compiled from
+the reference sources, oracle/_ref/ref_driver) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = ("setup columns/s on 1 B200: batched mixed vs plain FP64 at equal "
+          "‖AM−I‖_F")
+UNIT = "columns/s"
+BASE_SEED = 0x5EED0003
+REF_DRIVER = os.path.join(HERE, "oracle", "_ref", "ref_driver")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=1_000_000, help="columns per GPU")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(n):
+    return {"workload": f"ragged n={n} (U{{4..32}} off-diagonals, pattern(A^2) dropped 1e-3), "
+                        "fixed pattern, B = I",
+            "columns_per_gpu": n, "pattern": "A^2 drop 1e-3", "ns": 0,
+            "l2": "inputs larger than L2 (A and P are ~230 MB and ~540 MB at n=1e6)"}
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ reference arm helpers
+def write_subproblem(w, cols, directory):
+    """Matrix Market files of the sub-problem that columns [0, cols) see.
+
+    Columns of A outside the union of J_k (k < cols) are replaced by unit
+    columns (never read by those columns' least-squares problems: ns = 0);
+    the pattern keeps J_k for k < cols and is diagonal elsewhere.  The
+    reference therefore computes exactly the columns [0, cols) of the full
+    setup."""
+    import scipy.sparse as sp
+    from mspai_b200 import workloads as W
+    A = sp.csc_matrix(w.A)
+    P = sp.csc_matrix(w.P)
+    n = A.shape[1]
+    used = np.unique(P.indices[: P.indptr[cols]])
+    keep = np.zeros(n, dtype=bool)
+    keep[used] = True
+    lens = np.diff(A.indptr)
+    colmask = np.repeat(keep, lens)
+    rows_kept = A.indices[colmask]
+    cols_kept = np.repeat(np.arange(n), lens)[colmask]
+    vals_kept = A.data[colmask]
+    other = np.nonzero(~keep)[0]
+    Asub = sp.csc_matrix((np.concatenate([vals_kept, np.ones(len(other))]),
+                          (np.concatenate([rows_kept, other]), np.concatenate([cols_kept, other]))),
+                         shape=(n, n))
+    prow = np.concatenate([P.indices[: P.indptr[cols]], np.arange(cols, n)])
+    pcol = np.concatenate([np.repeat(np.arange(cols), np.diff(P.indptr)[:cols]), np.arange(cols, n)])
+    Psub = sp.csc_matrix((np.ones(len(prow)), (prow, pcol)), shape=(n, n))
+    W.write_mm(os.path.join(directory, "A.mtx"), Asub)
+    W.write_mm(os.path.join(directory, "P.mtx"), Psub, pattern=True)
+
+
+def run_reference_sample(directory, lo, hi, tag):
+    """Times the reference's SPAI_Column loop on columns [lo, hi) (1 thread)."""
+    env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS="1")
+    tfile = os.path.join(directory, f"t_{tag}.json")
+    return subprocess.Popen([REF_DRIVER, "A.mtx", "P.mtx", "-1", "-ns", "0", "-cols",
+                             f"{lo}:{hi}", "-time", tfile, "-out", f"M_{tag}.mtx"],
+                            cwd=directory, env=env, stdout=subprocess.DEVNULL,
+                            stderr=subprocess.DEVNULL), tfile
+
+
+def cpu_reference_rate(w, cols_per_proc, procs, directory, write=True):
+    """columns/s of the reference on `procs` host cores (one process each)."""
+    if write:
+        write_subproblem(w, cols_per_proc * procs, directory)
+    jobs = []
+    for p in range(procs):
+        jobs.append(run_reference_sample(directory, p * cols_per_proc, (p + 1) * cols_per_proc, p))
+    secs = []
+    for proc, tfile in jobs:
+        if proc.wait() != 0:
+            raise RuntimeError("reference driver failed")
+        secs.append(json.load(open(tfile))["setup_s"])
+    return cols_per_proc * procs / max(secs), max(secs)
+
+
+def oracle_port_rate(w, cols):
+    from oracle import pyoracle
+    t0 = time.perf_counter()
+    pyoracle.spai_scalar(w.A, w.P, ns=0, cols=(0, cols))
+    dt = time.perf_counter() - t0
+    return cols / dt, dt
+
+
+# ------------------------------------------------------------------ main paths
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def bench_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    if not os.path.exists(REF_DRIVER):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/ref_driver was not built (needs the "
+                                         "reference sources at build time)"}))
+        return 0
+    from mspai_b200 import workloads as W
+    w = W.ragged(args.n, seed=BASE_SEED)
+    procs = max(1, os.cpu_count() or 1)
+    per = 4
+    with tempfile.TemporaryDirectory() as d:
+        write_subproblem(w, per * procs, d)
+        for _ in range(args.warmup):
+            cpu_reference_rate(w, per, procs, d, write=False)
+        rates, secs = [], []
+        for _ in range(args.steps):
+            r, s = cpu_reference_rate(w, per, procs, d, write=False)
+            rates.append(r)
+            secs.append(s)
+    value = float(np.median(rates))
+    sample = (f"columns [0, {per * procs}) of the {args.n}-column workload, {per} per process, "
+              f"{procs} processes (OPENBLAS_NUM_THREADS=1), reference SPAI_Column loop")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": float(np.median(secs)) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args.n),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+    return 0
+
+
+def bench_ours(args):
+    import torch
+    import mspai_b200 as mb
+    from mspai_b200 import workloads as W
+
+    world, rank, local = dist_setup(args)
+    n = args.n
+    w = W.ragged(n, seed=BASE_SEED + rank)
+    stream = torch.cuda.current_stream()
+    h = mb.Handle(local, stream=stream.cuda_stream)
+    dA = mb.DeviceCSC.from_scipy(w.A)
+    dP = mb.DeviceCSC.from_scipy(w.P, pattern=True)
+    torch.cuda.synchronize()
+    mixed = mb.Options(ns=0, prec="mixed", refine=2, batched=True)
+
+    for _ in range(max(args.warmup, 3) if args.warmup >= 0 else 3):
+        h.setup(dA, dP, options=mixed)
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        h.setup(dA, dP, options=mixed)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    ms = max_over_ranks(ms, world)
+    value = world * n / (ms * 1e-3)
+    st = h.stats()
+    res_mixed, _, status_mixed = h.column_info()
+    frob_mixed = float(np.sqrt(np.sum(res_mixed ** 2)))
+
+    # roofline of the dominant kernel (largest bucket time)
+    b = int(np.argmax(st["kernel_ms"]))
+    kms = st["kernel_ms"][b]
+    achieved = st["bucket_flops"][b] / (kms * 1e-3) / 1e12 if kms > 0 else None
+    peak32 = mb.measure_fma_peak(local, fp64=False) / 1e3
+    traffic = None
+    prof = os.path.join(HERE, "profiles", "ragged_solve_traffic.json")
+    if os.path.exists(prof):
+        try:
+            pj = json.load(open(prof))
+            traffic = pj.get("dram_bytes_per_launch_scaled")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
+                "frac": (achieved / peak32) if achieved else None, "traffic": traffic,
+                "kernel": ["warp_solve", "cta_solve(W in smem)", "cta_solve(W in global)"][b],
+                "kernel_ms": kms, "flops_per_launch": st["bucket_flops"][b],
+                "peak_source": "measured FP32 FMA probe (mspai_measure_fma_peak)"}
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded, shapes of the "
+        "ragged 1M-column configuration)", "config": workload_config(n),
+        "roofline": roofline, "clocks": clocks,
+        "gpu_launches": int(st["kernel_launches"]) * args.steps,
+        "stats": {"buckets": st["bucket_columns"], "kernel_ms": st["kernel_ms"],
+                  "flops_folded": st["flops"], "flops_dense_equivalent": st["flops_dense"],
+                  "setup_ms_device": st["setup_ms"]},
+    }
+
+    # plain per-column FP64 GPU path (the metric's comparison) and the equal-F check
+    if not args.no_plain:
+        plain = mb.Options(ns=0, prec="fp64", batched=False)
+        h.setup(dA, dP, options=plain)
+        torch.cuda.synchronize()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        h.setup(dA, dP, options=plain)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        pms = max_over_ranks(p0.elapsed_time(p1), world)
+        res_plain, _, _ = h.column_info()
+        frob_plain = float(np.sqrt(np.sum(res_plain ** 2)))
+        out["plain_fp64"] = {"value": world * n / (pms * 1e-3), "unit": UNIT, "ms_per_step": pms,
+                             "speedup_of_mixed": (world * n / (ms * 1e-3)) /
+                                                 (world * n / (pms * 1e-3)),
+                             "frob_AM_minus_I_mixed": frob_mixed,
+                             "frob_AM_minus_I_fp64": frob_plain,
+                             "frob_rel_diff": abs(frob_mixed - frob_plain) / frob_plain}
+
+    # end to end through the public API from pinned host memory
+    if not args.no_e2e:
+        hA = mb.DeviceCSC.from_scipy(w.A, device="cpu", pin=True)
+        hP = mb.DeviceCSC.from_scipy(w.P, device="cpu", pattern=True, pin=True)
+        nnz_m = w.P.nnz
+        oc = torch.empty(n + 1, dtype=torch.int64).pin_memory()
+        oi = torch.empty(nnz_m, dtype=torch.int32).pin_memory()
+        ov = torch.empty(nnz_m, dtype=torch.float64).pin_memory()
+        h.setup(hA, hP, options=mixed)
+        h.result_into(oc.numpy(), oi.numpy(), ov.numpy())
+        barrier(world)
+        torch.cuda.synchronize()
+        ksteps = max(1, min(args.steps, 2))
+        q0 = torch.cuda.Event(enable_timing=True)
+        q1 = torch.cuda.Event(enable_timing=True)
+        q0.record(stream)
+        for _ in range(ksteps):
+            h.setup(hA, hP, options=mixed)
+            h.result_into(oc.numpy(), oi.numpy(), ov.numpy())
+        q1.record(stream)
+        torch.cuda.synchronize()
+        ems = max_over_ranks(q0.elapsed_time(q1) / ksteps, world)
+        out["e2e"] = {"value": world * n / (ems * 1e-3), "unit": UNIT,
+                      "h2d_bytes_per_step": hA.nbytes() + hP.nbytes(),
+                      "d2h_bytes_per_step": oc.numel() * 8 + oi.numel() * 4 + ov.numel() * 8,
+                      "ms_per_step": ems}
+
+    # CPU baseline: the reference's column loop on a bounded sample, 1 core
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            if os.path.exists(REF_DRIVER):
+                cols = 48
+                with tempfile.TemporaryDirectory() as d:
+                    rate, secs = cpu_reference_rate(w, cols, 1, d)
+                out["cpu_baseline"] = {
+                    "value": rate, "unit": UNIT, "cores": 1, "kind": "reference",
+                    "sample": f"columns [0, {cols}) of this workload, reference SPAI_Column "
+                              f"loop, 1 thread ({secs:.1f} s)"}
+            else:
+                cols = 48
+                rate, secs = oracle_port_rate(w, cols)
+                out["cpu_baseline"] = {
+                    "value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+                    "sample": f"columns [0, {cols}) via the oracle restatement ({secs:.1f} s)"}
+        except Exception as exc:  # the baseline is reported, never the target
+            out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
+                                   "sample": f"failed: {exc}"}
+    h.close()
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return bench_reference(args)
+    return bench_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -91,6 +92,7 @@ struct mspai_handle {
     mspai_stats stats{};
     mspai_params last_params{};
     int64_t launches = 0;
+    size_t smem_budget = 200 * 1024;  // shared-memory area of the CTA solver
 };
 
 static int set_err(mspai_handle* h, int code, const char* fmt, ...)
@@ -193,6 +195,11 @@ int mspai_create(mspai_handle** out, int32_t device, void* stream)
     cudaEventCreate(&h->ev1);
     for (auto& e : h->evb)
         cudaEventCreate(&e);
+    if (const char* kb = std::getenv("MSPAI_SMEM_KB")) {
+        const long v = std::atol(kb);
+        if (v >= 16 && v <= 220)
+            h->smem_budget = static_cast<size_t>(v) * 1024;
+    }
     *out = h;
     return MSPAI_OK;
 }
@@ -470,11 +477,17 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
                                                  &grid));
         }
         else {
-            const bool wsm = (b == 1) && mspai::w_bytes(cap, elem) <= 200 * 1024;
-            const size_t need = mspai::cta_scratch_needed(elem, wsm, cap, count);
+            // shared memory for the folded matrix: the bucket's worst case when
+            // it is small, else a large area (one CTA per SM) that holds W when
+            // it fits and stages the QR panels when it does not
+            size_t wsm = std::min<size_t>(mspai::w_bytes(cap, elem), h->smem_budget);
+            if (!prm->batched)
+                wsm = 0;  // the plain path keeps W in global memory, unblocked
+            const size_t need = mspai::cta_scratch_needed(elem, cap, count);
             CUDA_TRY(h, h->scratch.ensure(need));
             h->launches++;
-            CUDA_TRY(h, mspai::launch_cta_solve(elem, wsm, pb, cap, out, list, count, counter,
+            CUDA_TRY(h, mspai::launch_cta_solve(elem, wsm, prm->batched != 0, pb, cap, out, list,
+                                                count, counter,
                                                 h->scratch.as<char>(), h->scratch.bytes, st,
                                                 &grid));
         }

@@ -1,0 +1,451 @@
+// Blocked Householder QR and blocked triangular solves for one CTA.
+//
+// The folded least-squares matrix W (mw x n, column-major, ld = mw) lives in
+// shared memory when it fits, else in the CTA's global scratch slot.  The QR
+// follows LAPACK's dgeqrf: 16-column panels are factored with unblocked
+// Householder reflectors (dgeqr2), the panel's reflectors are accumulated into
+// the compact WY form H_0...H_{nb-1} = I - V T V^T (dlarft, forward,
+// columnwise), and the trailing columns plus the right-hand side are updated
+// as W2 <- W2 - V (T^T (V^T W2)) (dlarfb, transposed).  The trailing update is
+// a register-tiled mini-GEMM: one warp owns 4 trailing columns, lanes split
+// the rows, the 4 x 16 partial dot products are combined with a warp
+// reduce-scatter, and the rank-16 update reuses every V element for 4
+// columns.  When W is in global memory the panel is staged in shared memory,
+// so only the trailing update touches global memory (twice per panel instead
+// of twice per column).
+#pragma once
+
+#include "spai_device.cuh"
+
+namespace mspai {
+
+constexpr int kPanel = 16;     // panel width
+constexpr int kTileCols = 4;   // trailing columns per warp tile
+
+// Shared-memory scratch of the blocked routines (besides the W/panel area).
+template <class T>
+struct BlockedScratch {
+    T tmat[kPanel * kPanel];  // T factor (upper triangular, column-major)
+    T tau[kPanel];
+    T vtv[kPanel * kPanel];   // V^T V (strictly upper part used)
+};
+
+// V(r, i) of the panel: unit lower trapezoidal, explicit below the diagonal.
+template <class T>
+__device__ __forceinline__ T vpanel(const T* P, int ldp, int r, int i)
+{
+    const T v = P[r + static_cast<size_t>(i) * ldp];
+    return r > i ? v : (r == i ? T(1) : T(0));
+}
+
+// Unblocked Householder QR of the panel P (mp x nb, ld ldp); tau[k] = 0 when
+// the column below the diagonal is zero (H = I), as LAPACK's dlarfg.
+template <class T, class G>
+__device__ void panel_qr(const G& g, T* P, int ldp, int mp, int nb, T* tau)
+{
+    const int lane = g.lane();
+    for (int k = 0; k < nb; k++) {
+        T* pk = P + static_cast<size_t>(k) * ldp;
+        T part = 0;
+        for (int i = k + 1 + g.rank(); i < mp; i += G::kSize)
+            part += pk[i] * pk[i];
+        const T xnorm2 = g.sum(part);
+        if (xnorm2 == T(0) || k >= mp) {
+            if (g.rank() == 0)
+                tau[k] = T(0);
+            g.sync();
+            continue;
+        }
+        const T alpha = pk[k];
+        const T beta = -copysign(tsqrt<T>(alpha * alpha + xnorm2), alpha);
+        const T tk = (beta - alpha) / beta;
+        const T scale = T(1) / (alpha - beta);
+        g.sync();
+        if (g.rank() == 0) {
+            pk[k] = beta;
+            tau[k] = tk;
+        }
+        for (int i = k + 1 + g.rank(); i < mp; i += G::kSize)
+            pk[i] *= scale;
+        g.sync();
+        for (int c = k + 1 + g.warp(); c < nb; c += G::kWarps) {
+            T* col = P + static_cast<size_t>(c) * ldp;
+            T d = (lane == 0) ? col[k] : T(0);
+            for (int i = k + 1 + lane; i < mp; i += 32)
+                d += pk[i] * col[i];
+            d = warp_sum(d) * tk;
+            if (lane == 0)
+                col[k] -= d;
+            for (int i = k + 1 + lane; i < mp; i += 32)
+                col[i] -= d * pk[i];
+        }
+        g.sync();
+    }
+}
+
+// T factor of the panel (dlarft, forward, columnwise):
+//   T(k,k) = tau_k,  T(0:k, k) = -tau_k T(0:k, 0:k) V(:, 0:k)^T v_k.
+template <class T, class G>
+__device__ void panel_tfactor(const G& g, const T* P, int ldp, int mp, int nb,
+                              BlockedScratch<T>* bs)
+{
+    // V^T V for j < k: (j, k) pairs spread over the warps, lanes over rows >= k
+    const int lane = g.lane();
+    const int pairs = nb * (nb - 1) / 2;
+    for (int q = g.warp(); q < pairs; q += G::kWarps) {
+        // decode q -> (j, k), j < k
+        int k = 1, base = 0;
+        while (base + k <= q) {
+            base += k;
+            k++;
+        }
+        const int j = q - base;
+        T d = 0;
+        for (int r = k + lane; r < mp; r += 32)
+            d += vpanel(P, ldp, r, j) * vpanel(P, ldp, r, k);
+        d = warp_sum(d);
+        if (lane == 0)
+            bs->vtv[j + k * kPanel] = d;
+    }
+    g.sync();
+    if (g.warp() == 0) {
+        for (int k = 0; k < nb; k++) {
+            const T tk = bs->tau[k];
+            // T(i, k) for i < k: -tau_k sum_{j=i}^{k-1} T(i, j) vtv(j, k)
+            T v = 0;
+            if (lane < k) {
+                for (int j = lane; j < k; j++)
+                    v += bs->tmat[lane + j * kPanel] * bs->vtv[j + k * kPanel];
+                v = -tk * v;
+            }
+            __syncwarp();
+            if (lane < k)
+                bs->tmat[lane + k * kPanel] = v;
+            if (lane == k)
+                bs->tmat[k + k * kPanel] = tk;
+            if (lane > k && lane < kPanel)
+                bs->tmat[lane + k * kPanel] = T(0);
+            __syncwarp();
+        }
+    }
+    g.sync();
+}
+
+// Trailing update of `ncols` columns starting at W2 (ld ldw, rows aligned with
+// the panel's rows) plus the right-hand side `rhs2` (treated as column ncols):
+//   X <- X - V (T^T (V^T X)).
+template <class T, class G>
+__device__ void trailing_update(const G& g, const T* P, int ldp, int mp, int nb,
+                                const BlockedScratch<T>* bs, T* W2, int ldw, int ncols, T* rhs2)
+{
+    const int lane = g.lane();
+    const int total = ncols + 1;
+    for (int cb = g.warp() * kTileCols; cb < total; cb += G::kWarps * kTileCols) {
+        T* col[kTileCols];
+#pragma unroll
+        for (int c = 0; c < kTileCols; c++) {
+            const int cc = cb + c;
+            col[c] = (cc < ncols) ? W2 + static_cast<size_t>(cc) * ldw : (cc == ncols ? rhs2 : nullptr);
+        }
+        // Y = V^T X (partial sums per lane over its rows).  Rows are taken four
+        // at a time so that 16 independent loads of X are in flight per lane
+        // (X may be in global memory).
+        T acc[kTileCols * kPanel];
+#pragma unroll
+        for (int t = 0; t < kTileCols * kPanel; t++)
+            acc[t] = T(0);
+        constexpr int kRows = 4;
+        int r0 = lane;
+        for (; r0 + 32 * (kRows - 1) < mp; r0 += 32 * kRows) {
+            T x[kRows][kTileCols];
+#pragma unroll
+            for (int q = 0; q < kRows; q++)
+#pragma unroll
+                for (int c = 0; c < kTileCols; c++)
+                    x[q][c] = col[c] ? col[c][r0 + 32 * q] : T(0);
+#pragma unroll
+            for (int q = 0; q < kRows; q++) {
+                const int r = r0 + 32 * q;
+#pragma unroll
+                for (int i = 0; i < kPanel; i++) {
+                    const T v = (i < nb) ? vpanel(P, ldp, r, i) : T(0);
+#pragma unroll
+                    for (int c = 0; c < kTileCols; c++)
+                        acc[c * kPanel + i] += v * x[q][c];
+                }
+            }
+        }
+        for (int r = r0; r < mp; r += 32) {
+            T x[kTileCols];
+#pragma unroll
+            for (int c = 0; c < kTileCols; c++)
+                x[c] = col[c] ? col[c][r] : T(0);
+#pragma unroll
+            for (int i = 0; i < kPanel; i++) {
+                const T v = (i < nb) ? vpanel(P, ldp, r, i) : T(0);
+#pragma unroll
+                for (int c = 0; c < kTileCols; c++)
+                    acc[c * kPanel + i] += v * x[c];
+            }
+        }
+        // warp reduce-scatter: lane l ends with the sums of entries 2l, 2l+1
+#pragma unroll
+        for (int level = 0; level < 5; level++) {
+            const int half = (kTileCols * kPanel) >> (level + 1);
+            const int bit = 16 >> level;
+            const bool upper = (lane & bit) != 0;
+#pragma unroll
+            for (int t = 0; t < 32; t++) {
+                if (t < half) {
+                    const T mine = upper ? acc[half + t] : acc[t];
+                    const T other = upper ? acc[t] : acc[half + t];
+                    acc[t] = mine + __shfl_xor_sync(0xffffffffu, other, bit);
+                }
+            }
+        }
+        // Y entries 2*lane, 2*lane+1 -> Z = T^T Y via shared exchange of Y
+        __shared__ T ybuf_all[G::kWarps][kTileCols * kPanel];  // one row per warp
+        T* ybuf = ybuf_all[g.warp()];
+        ybuf[2 * lane] = acc[0];
+        ybuf[2 * lane + 1] = acc[1];
+        __syncwarp();
+        T z2[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int idx = 2 * lane + h;
+            const int c = idx / kPanel, i = idx % kPanel;
+            T z = 0;
+            for (int j = 0; j <= i && j < nb; j++)
+                z += bs->tmat[j + i * kPanel] * ybuf[c * kPanel + j];
+            z2[h] = (i < nb) ? z : T(0);
+        }
+        __syncwarp();
+        ybuf[2 * lane] = z2[0];
+        ybuf[2 * lane + 1] = z2[1];
+        __syncwarp();
+        T zr[kTileCols * kPanel];
+#pragma unroll
+        for (int t = 0; t < kTileCols * kPanel; t++)
+            zr[t] = ybuf[t];
+        // X -= V Z (four rows per lane at a time: loads first, then stores)
+        int r1 = lane;
+        for (; r1 + 32 * (kRows - 1) < mp; r1 += 32 * kRows) {
+            T x[kRows][kTileCols];
+#pragma unroll
+            for (int q = 0; q < kRows; q++)
+#pragma unroll
+                for (int c = 0; c < kTileCols; c++)
+                    x[q][c] = col[c] ? col[c][r1 + 32 * q] : T(0);
+#pragma unroll
+            for (int q = 0; q < kRows; q++) {
+                const int r = r1 + 32 * q;
+#pragma unroll
+                for (int i = 0; i < kPanel; i++) {
+                    const T v = (i < nb) ? vpanel(P, ldp, r, i) : T(0);
+#pragma unroll
+                    for (int c = 0; c < kTileCols; c++)
+                        x[q][c] -= v * zr[c * kPanel + i];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kRows; q++)
+#pragma unroll
+                for (int c = 0; c < kTileCols; c++)
+                    if (col[c])
+                        col[c][r1 + 32 * q] = x[q][c];
+        }
+        for (int r = r1; r < mp; r += 32) {
+            T x[kTileCols];
+#pragma unroll
+            for (int c = 0; c < kTileCols; c++)
+                x[c] = col[c] ? col[c][r] : T(0);
+#pragma unroll
+            for (int i = 0; i < kPanel; i++) {
+                const T v = (i < nb) ? vpanel(P, ldp, r, i) : T(0);
+#pragma unroll
+                for (int c = 0; c < kTileCols; c++)
+                    x[c] -= v * zr[c * kPanel + i];
+            }
+#pragma unroll
+            for (int c = 0; c < kTileCols; c++)
+                if (col[c])
+                    col[c][r] = x[c];
+        }
+        __syncwarp();
+    }
+}
+
+// Blocked Householder QR of W (mw x n, ld) applied to rhs.  `region` is a
+// shared-memory area of at least mw * kPanel elements used to stage panels
+// when W is not itself in shared memory (w_in_smem == false).
+template <class T, class G>
+__device__ void group_householder_blocked(const G& g, T* W, int ld, int mw, int n, T* rhs,
+                                          bool w_in_smem, T* region, BlockedScratch<T>* bs)
+{
+    const int kmax = min(mw, n);
+    for (int c0 = 0; c0 < kmax; c0 += kPanel) {
+        const int nb = min(kPanel, kmax - c0);
+        const int mp = mw - c0;
+        T* P;
+        int ldp;
+        T* Wc = W + static_cast<size_t>(c0) * ld + c0;
+        if (w_in_smem) {
+            P = Wc;
+            ldp = ld;
+        }
+        else {
+            P = region;
+            ldp = mp;
+            for (int t = g.rank(); t < mp * nb; t += G::kSize) {
+                const int c = t / mp, r = t - c * mp;
+                P[r + c * mp] = Wc[r + static_cast<size_t>(c) * ld];
+            }
+            g.sync();
+        }
+        panel_qr<T>(g, P, ldp, mp, nb, bs->tau);
+        panel_tfactor<T>(g, P, ldp, mp, nb, bs);
+        if (!w_in_smem) {
+            // only R (rows < nb of the panel) is needed later
+            for (int t = g.rank(); t < nb * nb; t += G::kSize) {
+                const int c = t / nb, r = t - c * nb;
+                if (r <= c)
+                    Wc[r + static_cast<size_t>(c) * ld] = P[r + c * mp];
+            }
+        }
+        trailing_update<T>(g, P, ldp, mp, nb, bs, W + static_cast<size_t>(c0 + nb) * ld + c0, ld,
+                           n - c0 - nb, rhs + c0);
+        g.sync();
+    }
+}
+
+// Read-only view of the triangular factor R: column-major with leading
+// dimension ld, or packed by columns (R(i, j) at j (j + 1) / 2 + i) when ld == 0.
+template <class T>
+struct RView {
+    const T* p;
+    int ld;
+    __device__ __forceinline__ T operator()(int i, int j) const
+    {
+        return ld > 0 ? p[static_cast<size_t>(j) * ld + i]
+                      : p[static_cast<size_t>(j) * (j + 1) / 2 + i];
+    }
+};
+
+// Copies the upper triangle of W (n x n part, ld) into `dst` packed by columns.
+template <class T, class G>
+__device__ void group_pack_r(const G& g, const T* W, int ld, int n, T* dst)
+{
+    const int total = n * (n + 1) / 2;
+    for (int t = g.rank(); t < total; t += G::kSize) {
+        // invert t = j (j + 1) / 2 + i, 0 <= i <= j
+        int j = static_cast<int>((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
+        while (j * (j + 1) / 2 > t)
+            j--;
+        while ((j + 1) * (j + 2) / 2 <= t)
+            j++;
+        const int i = t - j * (j + 1) / 2;
+        dst[t] = W[static_cast<size_t>(j) * ld + i];
+    }
+    g.sync();
+}
+
+// Back substitution R y = rhs(0:n) (R = upper triangle of W), blocked by 16
+// columns from the right; x (FP64) receives y.  Returns (uniformly) 1 if R has
+// a zero diagonal, in which case x = rhs(0:n) unchanged (LAPACK dtrtrs).
+template <class T, class G>
+__device__ int group_back_substitute_blocked(const G& g, RView<T> R, int n, T* rhs, double* x)
+{
+    int singular = 0;
+    for (int j = g.rank(); j < n; j += G::kSize)
+        if (R(j, j) == T(0))
+            singular = 1;
+    singular = g.sum(singular) > 0;
+    if (!singular) {
+        const int lane = g.lane();
+        for (int c1 = n; c1 > 0; c1 -= kPanel) {
+            const int c0 = max(0, c1 - kPanel);
+            if (g.warp() == 0) {
+                for (int j = c1 - 1; j >= c0; j--) {
+                    const T xj = rhs[j] / R(j, j);
+                    __syncwarp();
+                    if (lane == 0)
+                        rhs[j] = xj;
+                    for (int i = c0 + lane; i < j; i += 32)
+                        rhs[i] -= R(i, j) * xj;
+                    __syncwarp();
+                }
+            }
+            g.sync();
+            for (int i = g.rank(); i < c0; i += G::kSize) {
+                T s = 0;
+                for (int j = c0; j < c1; j++)
+                    s += R(i, j) * rhs[j];
+                rhs[i] -= s;
+            }
+            g.sync();
+        }
+    }
+    for (int j = g.rank(); j < n; j += G::kSize)
+        x[j] = static_cast<double>(rhs[j]);
+    g.sync();
+    return singular;
+}
+
+// gv <- R^-1 R^-T gv (FP64 accumulation, R in T), blocked by 16 columns.
+template <class T, class G>
+__device__ void group_normal_correction_blocked(const G& g, RView<T> R, int n, double* gv)
+{
+    const int lane = g.lane();
+    // forward R^T z = g
+    for (int c0 = 0; c0 < n; c0 += kPanel) {
+        const int c1 = min(n, c0 + kPanel);
+        for (int j = c0 + g.warp(); j < c1; j += G::kWarps) {
+            double d = 0.0;
+            for (int i = lane; i < c0; i += 32)
+                d += static_cast<double>(R(i, j)) * gv[i];
+            d = warp_sum(d);
+            if (lane == 0)
+                gv[j] -= d;
+        }
+        g.sync();
+        if (g.warp() == 0) {
+            for (int j = c0; j < c1; j++) {
+                double d = 0.0;
+                for (int i = c0 + lane; i < j; i += 32)
+                    d += static_cast<double>(R(i, j)) * gv[i];
+                d = warp_sum(d);
+                const double zj = (gv[j] - d) / static_cast<double>(R(j, j));
+                __syncwarp();
+                if (lane == 0)
+                    gv[j] = zj;
+                __syncwarp();
+            }
+        }
+        g.sync();
+    }
+    // backward R delta = z
+    for (int c1 = n; c1 > 0; c1 -= kPanel) {
+        const int c0 = max(0, c1 - kPanel);
+        if (g.warp() == 0) {
+            for (int j = c1 - 1; j >= c0; j--) {
+                const double dj = gv[j] / static_cast<double>(R(j, j));
+                __syncwarp();
+                if (lane == 0)
+                    gv[j] = dj;
+                for (int i = c0 + lane; i < j; i += 32)
+                    gv[i] -= static_cast<double>(R(i, j)) * dj;
+                __syncwarp();
+            }
+        }
+        g.sync();
+        for (int i = g.rank(); i < c0; i += G::kSize) {
+            double s2 = 0.0;
+            for (int j = c0; j < c1; j++)
+                s2 += static_cast<double>(R(i, j)) * gv[j];
+            gv[i] -= s2;
+        }
+        g.sync();
+    }
+}
+
+}  // namespace mspai

@@ -38,6 +38,19 @@ __device__ __forceinline__ int warp_sum(int v)
     return v;
 }
 
+template <class T>
+__device__ __forceinline__ T tsqrt(T v);
+template <>
+__device__ __forceinline__ float tsqrt<float>(float v)
+{
+    return sqrtf(v);
+}
+template <>
+__device__ __forceinline__ double tsqrt<double>(double v)
+{
+    return sqrt(v);
+}
+
 // Shared scratch a group needs for reductions and broadcasts.
 struct GroupScratch {
     double red[32];

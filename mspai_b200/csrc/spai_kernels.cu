@@ -22,6 +22,18 @@
 
 namespace mspai {
 
+#ifdef MSPAI_PHASE_TIMERS
+extern "C" int mspai_profile_phase_cycles(unsigned long long* out, int reset)
+{
+    cudaMemcpyFromSymbol(out, g_phase_cycles, sizeof(unsigned long long) * 16);
+    if (reset) {
+        unsigned long long z[16] = {};
+        cudaMemcpyToSymbol(g_phase_cycles, z, sizeof(z));
+    }
+    return 0;
+}
+#endif
+
 // ------------------------------------------------------------------ planning
 __global__ void plan_kernel(const int64_t* __restrict__ cptr, const int64_t* __restrict__ pptr,
                             const int32_t* __restrict__ pidx, int n, int32_t* __restrict__ E,
@@ -98,17 +110,21 @@ __global__ void __launch_bounds__(kWarpKernelThreads)
     }
 }
 
-template <class T, int NT, bool W_SMEM>
+template <class T, int NT>
 __global__ void __launch_bounds__(NT)
     cta_solve_kernel(Problem pb, Caps cap, Output out, const int32_t* __restrict__ list, int count,
-                     int32_t* __restrict__ counter, char* __restrict__ scratch, size_t slot_bytes)
+                     int32_t* __restrict__ counter, char* __restrict__ scratch, size_t slot_bytes,
+                     int wfast_elems, int blocked)
 {
     extern __shared__ __align__(16) char smem[];
     __shared__ GroupScratch sc;
+    __shared__ BlockedScratch<T> bsc;
     CtaGroup<NT> g{&sc};
-    SlotLayout<T> lay(cap, W_SMEM);
-    Slot<T> s = lay.at(scratch + static_cast<size_t>(blockIdx.x) * slot_bytes,
-                       W_SMEM ? reinterpret_cast<T*>(smem) : nullptr);
+    SlotLayout<T> lay(cap, false);
+    Slot<T> s = lay.at(scratch + static_cast<size_t>(blockIdx.x) * slot_bytes, nullptr);
+    s.Wfast = wfast_elems > 0 ? reinterpret_cast<T*>(smem) : nullptr;
+    s.wfast_elems = wfast_elems;
+    s.bsc = blocked ? &bsc : nullptr;
     while (true) {
         if (threadIdx.x == 0)
             sc.i[5] = atomicAdd(counter, 1);
@@ -301,21 +317,20 @@ cudaError_t launch_warp_solve(int elem_bytes, const Problem& pb, const Caps& cap
     return launch_warp_t<double>(pb, cap, out, list, count, counter, st, grid_out);
 }
 
-template <class T, int NT, bool WS>
+template <class T, int NT>
 static cudaError_t launch_cta_t(const Problem& pb, const Caps& cap, const Output& out,
                                 const int32_t* list, int count, int32_t* counter, char* scratch,
-                                size_t scratch_bytes, cudaStream_t st, int* grid_out)
+                                size_t scratch_bytes, size_t smem, int blocked, cudaStream_t st,
+                                int* grid_out)
 {
-    const size_t slot = SlotLayout<T>(cap, WS).bytes;
-    const size_t smem = WS ? w_bytes(cap, sizeof(T)) : 0;
-    cudaError_t e = cudaFuncSetAttribute(cta_solve_kernel<T, NT, WS>,
+    const size_t slot = SlotLayout<T>(cap, false).bytes;
+    cudaError_t e = cudaFuncSetAttribute(cta_solve_kernel<T, NT>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess)
         return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cta_solve_kernel<T, NT, WS>, NT,
-                                                      smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cta_solve_kernel<T, NT>, NT, smem);
     if (e != cudaSuccess)
         return e;
     if (per_sm < 1)
@@ -327,32 +342,31 @@ static cudaError_t launch_cta_t(const Problem& pb, const Caps& cap, const Output
         return cudaErrorMemoryAllocation;
     grid = static_cast<int>(std::min<size_t>(grid, slots_fit));
     *grid_out = grid;
-    cta_solve_kernel<T, NT, WS><<<grid, NT, smem, st>>>(pb, cap, out, list, count, counter,
-                                                        scratch, slot);
+    const int wfast = static_cast<int>(smem / sizeof(T));
+    cta_solve_kernel<T, NT><<<grid, NT, smem, st>>>(pb, cap, out, list, count, counter, scratch,
+                                                    slot, wfast, blocked);
     return cudaGetLastError();
 }
 
-cudaError_t launch_cta_solve(int elem_bytes, bool w_smem, const Problem& pb, const Caps& cap,
-                             const Output& out, const int32_t* list, int count, int32_t* counter,
-                             char* scratch, size_t scratch_bytes, cudaStream_t st, int* grid_out)
+cudaError_t launch_cta_solve(int elem_bytes, size_t smem_w_bytes, bool blocked,
+                             const Problem& pb, const Caps& cap, const Output& out,
+                             const int32_t* list, int count, int32_t* counter, char* scratch,
+                             size_t scratch_bytes, cudaStream_t st, int* grid_out)
 {
-    if (elem_bytes == 4) {
-        if (w_smem)
-            return launch_cta_t<float, 128, true>(pb, cap, out, list, count, counter, scratch,
-                                                  scratch_bytes, st, grid_out);
-        return launch_cta_t<float, 256, false>(pb, cap, out, list, count, counter, scratch,
-                                               scratch_bytes, st, grid_out);
-    }
-    if (w_smem)
-        return launch_cta_t<double, 128, true>(pb, cap, out, list, count, counter, scratch,
-                                               scratch_bytes, st, grid_out);
-    return launch_cta_t<double, 128, false>(pb, cap, out, list, count, counter, scratch,
-                                            scratch_bytes, st, grid_out);
+    if (elem_bytes == 4)
+        return launch_cta_t<float, 256>(pb, cap, out, list, count, counter, scratch,
+                                        scratch_bytes, smem_w_bytes, blocked ? 1 : 0, st,
+                                        grid_out);
+    if (blocked)
+        return launch_cta_t<double, 256>(pb, cap, out, list, count, counter, scratch,
+                                         scratch_bytes, smem_w_bytes, 1, st, grid_out);
+    return launch_cta_t<double, 128>(pb, cap, out, list, count, counter, scratch, scratch_bytes,
+                                     smem_w_bytes, 0, st, grid_out);
 }
 
-size_t cta_scratch_needed(int elem_bytes, bool w_smem, const Caps& cap, int count)
+size_t cta_scratch_needed(int elem_bytes, const Caps& cap, int count)
 {
-    const size_t slot = cta_slot_bytes(cap, elem_bytes, w_smem);
+    const size_t slot = cta_slot_bytes(cap, elem_bytes, false);
     const size_t slots = static_cast<size_t>(std::min(count, 4 * num_sms()));
     return slot * std::max<size_t>(slots, 1);
 }

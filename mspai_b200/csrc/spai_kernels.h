@@ -33,13 +33,17 @@ cudaError_t launch_bucket(const int32_t* E, const int32_t* nk, int n, const Buck
 size_t warp_slot_bytes(const Caps& cap, int elem_bytes);
 size_t cta_slot_bytes(const Caps& cap, int elem_bytes, bool w_smem);
 size_t w_bytes(const Caps& cap, int elem_bytes);
-size_t cta_scratch_needed(int elem_bytes, bool w_smem, const Caps& cap, int count);
+size_t cta_scratch_needed(int elem_bytes, const Caps& cap, int count);
 cudaError_t launch_warp_solve(int elem_bytes, const Problem& pb, const Caps& cap,
                               const Output& out, const int32_t* list, int count, int32_t* counter,
                               cudaStream_t st, int* grid_out);
-cudaError_t launch_cta_solve(int elem_bytes, bool w_smem, const Problem& pb, const Caps& cap,
-                             const Output& out, const int32_t* list, int count, int32_t* counter,
-                             char* scratch, size_t scratch_bytes, cudaStream_t st, int* grid_out);
+// One CTA per column; the folded matrix of a column lives in `smem_w_bytes`
+// of shared memory when it fits there, else in the CTA's global scratch slot.
+// `blocked` selects the blocked Householder QR (16-column panels).
+cudaError_t launch_cta_solve(int elem_bytes, size_t smem_w_bytes, bool blocked,
+                             const Problem& pb, const Caps& cap, const Output& out,
+                             const int32_t* list, int count, int32_t* counter, char* scratch,
+                             size_t scratch_bytes, cudaStream_t st, int* grid_out);
 cudaError_t launch_scan_lengths(const int32_t* len, int n, int64_t* ptr, int64_t* tmp,
                                 cudaStream_t st);
 cudaError_t launch_capacity_len(const int64_t* pptr, int n, int grow, int32_t* len,

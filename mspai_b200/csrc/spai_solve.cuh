@@ -27,9 +27,31 @@
 //        rho <= bound; keep J sorted.
 #pragma once
 
+#include "spai_blocked.cuh"
 #include "spai_device.cuh"
 
 namespace mspai {
+
+// Optional per-phase cycle counters (profiling builds only: -DMSPAI_PHASE_TIMERS).
+#ifdef MSPAI_PHASE_TIMERS
+static __device__ unsigned long long g_phase_cycles[16];
+#define PHASE_BEGIN() long long _ph_t = clock64()
+#define PHASE_MARK(k)                                                        \
+    do {                                                                     \
+        if (g.rank() == 0) {                                                 \
+            const long long _now = clock64();                                \
+            atomicAdd(&g_phase_cycles[k], static_cast<unsigned long long>(_now - _ph_t)); \
+            _ph_t = _now;                                                    \
+        }                                                                    \
+    } while (0)
+#else
+#define PHASE_BEGIN() \
+    do {              \
+    } while (0)
+#define PHASE_MARK(k) \
+    do {              \
+    } while (0)
+#endif
 
 // Read-only inputs of a setup (device pointers).
 struct Problem {
@@ -90,6 +112,10 @@ struct Slot {
     double* r;         // emax   residual on I (FP64)
     T* W;              // mwmax * nmax folded matrix (column-major, ld = mw)
     T* rhs;            // mwmax
+    T* Wfast;          // optional shared-memory area for W (+ rhs) ...
+    int wfast_elems;   // ... used when mw * n + mw <= wfast_elems; otherwise
+                       // it stages the 16-column panels of the blocked QR
+    BlockedScratch<T>* bsc;  // shared scratch of the blocked QR (CTA groups)
     double* x;         // nmax  solution
     double* gv;        // nmax  refinement right-hand side / correction
     int32_t* cand;     // lcand candidate column indices (adaptive)
@@ -166,6 +192,9 @@ struct SlotLayout {
             s.W = reinterpret_cast<T*>(base + o_W);
         }
         s.rhs = nullptr;  // set by the caller from mw
+        s.Wfast = nullptr;
+        s.wfast_elems = 0;
+        s.bsc = nullptr;
         return s;
     }
 };
@@ -200,19 +229,6 @@ __device__ __forceinline__ int lower_bound_i32(const int32_t* a, int len, int v)
             hi = mid;
     }
     return lo;
-}
-
-template <class T>
-__device__ __forceinline__ T tsqrt(T v);
-template <>
-__device__ __forceinline__ float tsqrt<float>(float v)
-{
-    return sqrtf(v);
-}
-template <>
-__device__ __forceinline__ double tsqrt<double>(double v)
-{
-    return sqrt(v);
 }
 
 // Householder QR of W (mw x n, ld = mw) applied to rhs; R overwrites the upper
@@ -363,6 +379,7 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
         s.J[t] = pb.pidx[p0 + t];
     g.sync();
 
+    PHASE_BEGIN();
     for (int step = -1; step < pb.ns && status != 3; step++) {
         // ---- 1. entries of C(:, J), sorted by row
         for (int jj = g.rank(); jj < n; jj += G::kSize) {
@@ -395,8 +412,24 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
         for (int i = E + g.rank(); i < L; i += G::kSize)
             s.keys[i] = ~uint64_t(0);
         g.sync();
-        group_bitonic_sort(g, s.keys, L);
+        // sort in the CTA's shared area when it fits (it is free until W is
+        // built), else in place in the global slot
+        if (s.Wfast && static_cast<size_t>(L) * sizeof(uint64_t) <=
+                           static_cast<size_t>(s.wfast_elems) * sizeof(T)) {
+            uint64_t* ks = reinterpret_cast<uint64_t*>(s.Wfast);
+            for (int i = g.rank(); i < L; i += G::kSize)
+                ks[i] = s.keys[i];
+            g.sync();
+            group_bitonic_sort(g, ks, L);
+            for (int i = g.rank(); i < E; i += G::kSize)
+                s.keys[i] = ks[i];
+            g.sync();
+        }
+        else {
+            group_bitonic_sort(g, s.keys, L);
+        }
 
+        PHASE_MARK(0);
         // ---- unique rows I, positions of entries, row runs
         for (int i = g.rank(); i < E; i += G::kSize)
             s.tmp[i] = (i == 0 || (s.keys[i] >> kEntryBits) != (s.keys[i - 1] >> kEntryBits)) ? 1 : 0;
@@ -425,9 +458,15 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
             status = 3;
             break;
         }
-        T* W = s.W;
-        T* rhs = s.W + static_cast<size_t>(mw) * n;  // rhs directly after W
+        PHASE_MARK(1);
+        const bool w_smem = s.Wfast && mw * n + mw <= s.wfast_elems;
+        T* W = w_smem ? s.Wfast : s.W;
+        T* rhs = W + static_cast<size_t>(mw) * n;  // rhs directly after W
         const int ld = mw;
+        // blocked QR for CTA groups (panels staged in the shared area when W
+        // is in global memory and a panel fits there)
+        const bool blocked = (G::kWarps > 1) && s.bsc != nullptr &&
+                             (w_smem || (s.Wfast && mw * kPanel <= s.wfast_elems));
         for (int i = g.rank(); i < mw * n + mw; i += G::kSize)
             W[i] = T(0);
         g.sync();
@@ -463,9 +502,31 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
         }
         g.sync();
 
+        PHASE_MARK(2);
         // ---- 3. QR, Q^T b, back substitution
-        group_householder<T>(g, W, ld, mw, n, rhs);
-        const int sing = group_back_substitute<T>(g, W, ld, n, rhs, s.x);
+        int sing;
+        RView<T> rv{W, ld};
+        if (blocked) {
+            group_householder_blocked<T>(g, W, ld, mw, n, rhs, w_smem, s.Wfast, s.bsc);
+            if (!w_smem && static_cast<size_t>(n) * (n + 1) / 2 + n <=
+                               static_cast<size_t>(s.wfast_elems)) {
+                // R (packed) and the right-hand side move to shared memory
+                T* rp = s.Wfast;
+                T* rh = s.Wfast + static_cast<size_t>(n) * (n + 1) / 2;
+                group_pack_r<T>(g, W, ld, n, rp);
+                for (int i = g.rank(); i < n; i += G::kSize)
+                    rh[i] = rhs[i];
+                g.sync();
+                rv = RView<T>{rp, 0};
+                rhs = rh;
+            }
+            PHASE_MARK(3);
+            sing = group_back_substitute_blocked<T>(g, rv, n, rhs, s.x);
+        }
+        else {
+            group_householder<T>(g, W, ld, mw, n, rhs);
+            sing = group_back_substitute<T>(g, W, ld, n, rhs, s.x);
+        }
         steps++;
         if (g.rank() == 0) {
             const double dn = n, dmw = mw, dm = m;
@@ -476,6 +537,7 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
         }
         status = sing ? 1 : 0;
 
+        PHASE_MARK(4);
         // ---- 4/5. refinement (mixed) and FP64 residual
         double r2 = group_residual(g, pb, col, s.keys, s.I, s.rstart, s.ejj, s.ev, s.x,
                                    s.r, m);
@@ -491,7 +553,10 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
                         s.gv[jj] = d;
                 }
                 g.sync();
-                group_normal_correction<T>(g, W, ld, n, s.gv);
+                if (blocked)
+                    group_normal_correction_blocked<T>(g, rv, n, s.gv);
+                else
+                    group_normal_correction<T>(g, W, ld, n, s.gv);
                 for (int jj = g.rank(); jj < n; jj += G::kSize)
                     s.x[jj] += s.gv[jj];
                 g.sync();
@@ -501,6 +566,7 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
         }
         res = sqrt(r2);
         g.sync();
+        PHASE_MARK(5);
         if (res <= pb.ep || step == pb.ns - 1)
             break;
 
@@ -693,6 +759,7 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
             out.oidx[o0 + t] = s.J[t];
     }
     nonfinite = g.sum(nonfinite);
+    PHASE_MARK(6);
     if (g.rank() == 0) {
         out.olen[col] = n;
         out.res[col] = res;

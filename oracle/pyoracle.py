@@ -36,6 +36,11 @@ def load():
             ctypes.c_int, ctypes.c_int, P, P, P, P, P, P, P, P, P, P, P, P,
             ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
             ctypes.c_int, ctypes.c_int, P, P, P, P, P, P]
+        lib.oracle_spai_block.restype = ctypes.c_int
+        lib.oracle_spai_block.argtypes = [
+            ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, P, P, P, P, P, P, P,
+            ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+            ctypes.c_int, ctypes.c_int, P, P, P, P, P, P]
         _lib = lib
     return _lib
 
@@ -124,6 +129,70 @@ def spai_scalar(C: sp.csc_matrix, P: sp.csc_matrix, *, B: Optional[sp.csc_matrix
     sel = (np.arange(stride)[None, :] < lens[:, None]).ravel()
     M = sp.csc_matrix((out_val[sel], out_idx[sel], colptr), shape=(n, n))
     return OracleResult(M, out_res, out_steps, out_info)
+
+
+def spai_block(C: sp.csc_matrix, Pb: sp.csc_matrix, bs: int, *,
+               B: Optional[sp.csc_matrix] = None, ep: float = 0.4, mn: int = 5, ns: int = 5,
+               um: int = 1, blocks: Optional[tuple] = None) -> OracleResult:
+    """Block SPAI with constant block size bs; Pb is the (n/bs x n/bs) block pattern."""
+    lib = load()
+    C = sp.csc_matrix(C, dtype=np.float64)
+    C.sort_indices()
+    nrows, n = C.shape
+    cptr = np.ascontiguousarray(C.indptr, dtype=np.int64)
+    cidx = np.ascontiguousarray(C.indices, dtype=np.int32)
+    cval = np.ascontiguousarray(C.data, dtype=np.float64)
+    R = sp.csr_matrix(C[:n, :])
+    R.sort_indices()
+    rptr = np.ascontiguousarray(R.indptr, dtype=np.int64)
+    rcol = np.ascontiguousarray(R.indices, dtype=np.int32)
+    Pb = sp.csc_matrix(Pb)
+    Pb.sort_indices()
+    pptr = np.ascontiguousarray(Pb.indptr, dtype=np.int64)
+    pidx = np.ascontiguousarray(Pb.indices, dtype=np.int32)
+    bptr = bidx = bval = None
+    if B is not None:
+        B = sp.csc_matrix(B, dtype=np.float64)
+        B.sort_indices()
+        bptr = np.ascontiguousarray(B.indptr, dtype=np.int64)
+        bidx = np.ascontiguousarray(B.indices, dtype=np.int32)
+        bval = np.ascontiguousarray(B.data, dtype=np.float64)
+    nb = n // bs
+    lo, hi = (0, nb) if blocks is None else blocks
+    stride = bs * (int(np.diff(pptr).max()) + mn * ns) + 1
+    out_len = np.zeros(n, dtype=np.int32)
+    out_idx = np.zeros(n * stride, dtype=np.int32)
+    out_val = np.zeros(n * stride, dtype=np.float64)
+    out_res = np.zeros(n, dtype=np.float64)
+    out_steps = np.zeros(n, dtype=np.int32)
+    out_info = np.zeros(n, dtype=np.int32)
+    rc = lib.oracle_spai_block(nrows, n, bs, _ptr(cptr), _ptr(cidx), _ptr(cval), _ptr(rptr),
+                               _ptr(rcol), _ptr(bptr), _ptr(bidx), _ptr(bval), _ptr(pptr),
+                               _ptr(pidx), float(ep), int(mn), int(ns), int(um), int(lo),
+                               int(hi), stride, _ptr(out_len), _ptr(out_idx), _ptr(out_val),
+                               _ptr(out_res), _ptr(out_steps), _ptr(out_info))
+    if rc != 0:
+        raise RuntimeError(f"oracle failed ({rc})")
+    lens = out_len.astype(np.int64)
+    colptr = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(lens, out=colptr[1:])
+    sel = (np.arange(stride)[None, :] < lens[:, None]).ravel()
+    M = sp.csc_matrix((out_val[sel], out_idx[sel], colptr), shape=(n, n))
+    return OracleResult(M, out_res, out_steps, out_info)
+
+
+def block_pattern(A: sp.spmatrix, bs: int) -> sp.csc_matrix:
+    """Block pattern of A for a constant block size: block (I, J) present when
+    any scalar entry of A in it is stored (Matrix::Convert_Block_Matrix)."""
+    C = sp.coo_matrix(A)
+    nb = A.shape[1] // bs
+    keep = C.row < nb * bs
+    Pb = sp.coo_matrix((np.ones(int(keep.sum())), (C.row[keep] // bs, C.col[keep] // bs)),
+                       shape=(nb, nb)).tocsc()
+    Pb.sum_duplicates()
+    Pb.data[:] = 1.0
+    Pb.sort_indices()
+    return Pb
 
 
 def run_reference(args, cwd: str, timeout: float = 600.0) -> None:

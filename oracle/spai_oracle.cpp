@@ -298,4 +298,237 @@ int oracle_spai_scalar(int nrows, int n, const int64_t* cptr, const int32_t* cid
     return 0;
 }
 
+
+/*
+ * Block SPAI with a constant block size bs (Spai_Unrestrained_Block::
+ * SPAI_Column, src/Spai_Unrestrained_Block.imp:33-140), restated on the
+ * scalar CSC of C:
+ *   - block column kb has the scalar columns bs*kb .. bs*kb+bs-1; the block
+ *     pattern Pb gives J (block indices); I is the set of block rows that the
+ *     blocks of C(:, J) touch (rows >= n_s, probing rows, are single rows);
+ *   - A_hat = C(I, J) expanded to scalars (Create_Submatrix_AHat_Block,
+ *     src/Spai_Sub.imp:284-401), the right-hand side is the identity block at
+ *     block row kb (Create_ek_Hat_Block, :690-733) or B(I, bs*kb + c);
+ *   - dgeqrf / dormqr / dtrtrs with nrhs = bs (src/Spai_Unrestrained_Block.imp:
+ *     142-205), residual R = A_hat X - E and its Frobenius norm
+ *     (Residual_Norm_Block, src/Spai_Sub.imp:943-975), stop at ep * sqrt(bs);
+ *   - pattern update (Augment_Sparsity_Block, src/Spai_Sub.imp:1118-1229):
+ *     candidates are the block columns of the block rows of L = I u {kb},
+ *     rho_j^2 = ||R||_F^2 - <N, (A_j^T A_j)^-1 N> with N = A_j(I)^T R
+ *     (Compute_Rhos_Block :1350-1465, Compute_Numerator_Block
+ *     src/Spai_Sub.cpp:293-367; the inverse by dgetrf/dgetri as
+ *     Compute_Square_Inverse, src/Matrix.imp:2945-3030).
+ * Output: scalar column bs*kb + c of M holds rows expanded(J) and X(:, c).
+ */
+int oracle_spai_block(int nrows, int n_s, int bs, const int64_t* cptr, const int32_t* cidx,
+                      const double* cval, const int64_t* rptr, const int32_t* rcol,
+                      const int64_t* bptr, const int32_t* bidx, const double* bval,
+                      const int64_t* pbptr, const int32_t* pbidx, double ep, int mn, int ns,
+                      int um, int kb_lo, int kb_hi, int out_stride, int32_t* out_len,
+                      int32_t* out_idx, double* out_val, double* out_res, int32_t* out_steps,
+                      int32_t* out_info)
+{
+    const int nb = n_s / bs;
+    if (nb * bs != n_s)
+        return -1000000;
+    const int nblocks_rows = nb + (nrows - n_s);  // probing rows are blocks of one
+    auto row_block = [&](int r) { return r < n_s ? r / bs : nb + (r - n_s); };
+    auto block_first = [&](int b) { return b < nb ? b * bs : n_s + (b - nb); };
+    auto block_height = [&](int b) { return b < nb ? bs : 1; };
+    std::vector<char> mark(std::max(nblocks_rows, nb) + 1, 0);
+    std::vector<int> J, I, L, U, Jt, rowoff;
+    std::vector<double> Ahat, E, X, R;
+    std::vector<RhoIdx> rhos;
+    for (int kb = kb_lo; kb < kb_hi; kb++) {
+        J.assign(pbidx + pbptr[kb], pbidx + pbptr[kb + 1]);
+        double res = 1.0e50;
+        int steps = 0, info = 0;
+        const double ep_eff = ep * std::sqrt(static_cast<double>(bs));
+        int m = 0, n = 0;
+        for (int step = -1; step < ns; step++) {
+            // I: block rows touched by C(:, J)
+            I.clear();
+            for (int jb : J)
+                for (int c = jb * bs; c < jb * bs + bs; c++)
+                    for (int64_t p = cptr[c]; p < cptr[c + 1]; p++) {
+                        const int b = row_block(cidx[p]);
+                        if (!mark[b]) {
+                            mark[b] = 1;
+                            I.push_back(b);
+                        }
+                    }
+            std::sort(I.begin(), I.end());
+            for (int b : I)
+                mark[b] = 0;
+            rowoff.assign(I.size() + 1, 0);
+            for (size_t i = 0; i < I.size(); i++)
+                rowoff[i + 1] = rowoff[i] + block_height(I[i]);
+            m = rowoff[I.size()];
+            n = static_cast<int>(J.size()) * bs;
+            // A_hat (m x n, column-major): scatter each scalar column
+            Ahat.assign(static_cast<size_t>(m) * n, 0.0);
+            for (size_t jj = 0; jj < J.size(); jj++)
+                for (int a = 0; a < bs; a++) {
+                    const int c = J[jj] * bs + a;
+                    for (int64_t p = cptr[c]; p < cptr[c + 1]; p++) {
+                        const int r = cidx[p];
+                        const int b = row_block(r);
+                        const size_t q = std::lower_bound(I.begin(), I.end(), b) - I.begin();
+                        const int row = rowoff[q] + (r - block_first(b));
+                        Ahat[(jj * bs + a) * static_cast<size_t>(m) + row] = cval[p];
+                    }
+                }
+            // right-hand side E (m x bs)
+            E.assign(static_cast<size_t>(m) * bs, 0.0);
+            for (int cc = 0; cc < bs; cc++) {
+                const int col = kb * bs + cc;
+                if (bptr) {
+                    for (int64_t p = bptr[col]; p < bptr[col + 1]; p++) {
+                        const int r = bidx[p];
+                        const int b = row_block(r);
+                        const auto it = std::lower_bound(I.begin(), I.end(), b);
+                        if (it != I.end() && *it == b)
+                            E[cc * static_cast<size_t>(m) + rowoff[it - I.begin()] +
+                              (r - block_first(b))] = bval[p];
+                    }
+                }
+                else {
+                    const auto it = std::lower_bound(I.begin(), I.end(), kb);
+                    if (it != I.end() && *it == kb)
+                        E[cc * static_cast<size_t>(m) + rowoff[it - I.begin()] + cc] = 1.0;
+                }
+            }
+            X = E;
+            X.resize(std::max<size_t>(X.size(), static_cast<size_t>(n) * bs), 0.0);
+            info = ls_solve(Ahat, m, n, bs, X.data(), std::max(m, 1));
+            steps++;
+            // R = A_hat X - E (X's first n rows, ld m)
+            R = E;
+            {
+                const char* T = "N";
+                int lda = std::max(m, 1), ldb = std::max(m, 1), ldc = std::max(m, 1), nr = bs;
+                double alpha = 1.0, beta = -1.0;
+                if (m > 0 && n > 0)
+                    dgemm(T, T, &m, &nr, &n, &alpha, Ahat.data(), &lda, X.data(), &ldb, &beta,
+                          R.data(), &ldc);
+                else
+                    for (auto& v : R)
+                        v = -v;
+            }
+            double s2 = 0.0;
+            for (double v : R)
+                s2 += v * v;
+            res = std::sqrt(s2);
+            if (res <= ep_eff || step == ns - 1)
+                break;
+            // candidates: block columns of the block rows of L = I u {kb}
+            L.clear();
+            for (int b : I)
+                if (b < nb)
+                    L.push_back(b);
+            if (std::find(L.begin(), L.end(), kb) == L.end())
+                L.push_back(kb);
+            U.clear();
+            for (int l : L)
+                for (int r = l * bs; r < l * bs + bs; r++)
+                    for (int64_t p = rptr[r]; p < rptr[r + 1]; p++) {
+                        const int cb = rcol[p] / bs;
+                        if (!mark[cb]) {
+                            mark[cb] = 1;
+                            U.push_back(cb);
+                        }
+                    }
+            for (int c : U)
+                mark[c] = 0;
+            std::sort(U.begin(), U.end());
+            Jt.resize(U.size());
+            Jt.erase(std::set_difference(U.begin(), U.end(), J.begin(), J.end(), Jt.begin()),
+                     Jt.end());
+            if (Jt.empty())
+                break;
+            rhos.resize(Jt.size());
+            double mean = 0.0;
+            for (size_t t = 0; t < Jt.size(); t++) {
+                const int jb = Jt[t];
+                // N = A_j(I)^T R (bs x bs), G = A_j^T A_j (bs x bs, whole column)
+                std::vector<double> N(static_cast<size_t>(bs) * bs, 0.0), G(N.size(), 0.0);
+                for (int a = 0; a < bs; a++) {
+                    const int c = jb * bs + a;
+                    for (int64_t p = cptr[c]; p < cptr[c + 1]; p++) {
+                        const int r = cidx[p];
+                        const int b = row_block(r);
+                        const auto it = std::lower_bound(I.begin(), I.end(), b);
+                        if (it == I.end() || *it != b)
+                            continue;
+                        const int row = rowoff[it - I.begin()] + (r - block_first(b));
+                        for (int q = 0; q < bs; q++)
+                            N[a + q * bs] += cval[p] * R[q * static_cast<size_t>(m) + row];
+                    }
+                    for (int a2 = 0; a2 < bs; a2++) {
+                        const int c2 = jb * bs + a2;
+                        int64_t p = cptr[c], q = cptr[c2];
+                        double g = 0.0;
+                        while (p < cptr[c + 1] && q < cptr[c2 + 1]) {
+                            if (cidx[p] < cidx[q])
+                                p++;
+                            else if (cidx[p] > cidx[q])
+                                q++;
+                            else
+                                g += cval[p++] * cval[q++];
+                        }
+                        G[a + a2 * bs] = g;
+                    }
+                }
+                // G^-1 via dgetrf/dgetri (Compute_Square_Inverse)
+                {
+                    int nn = bs, lda = bs, inf = 0, lw = -1;
+                    std::vector<int> ipiv(bs);
+                    dgetrf_(&nn, &nn, G.data(), &lda, ipiv.data(), &inf);
+                    double wq = 0.0;
+                    dgetri_(&nn, G.data(), &lda, ipiv.data(), &wq, &lw, &inf);
+                    lw = std::max(1, static_cast<int>(wq));
+                    std::vector<double> wk(lw);
+                    dgetri_(&nn, G.data(), &lda, ipiv.data(), wk.data(), &lw, &inf);
+                }
+                double term = 0.0;
+                for (int q = 0; q < bs; q++)
+                    for (int a = 0; a < bs; a++) {
+                        double bm = 0.0;
+                        for (int a2 = 0; a2 < bs; a2++)
+                            bm += G[a + a2 * bs] * N[a2 + q * bs];
+                        term += bm * N[a + q * bs];
+                    }
+                double rho = std::sqrt(res * res - term);
+                mean += rho;
+                rhos[t].idx = jb;
+                rhos[t].rho = rho;
+            }
+            if (um)
+                mean /= static_cast<double>(Jt.size());
+            std::sort(rhos.begin(), rhos.end(), RhoLess());
+            for (int el = 0; el < mn && el < static_cast<int>(Jt.size()) && rhos[el].rho <= mean;
+                 el++)
+                J.push_back(rhos[el].idx);
+            std::sort(J.begin(), J.end());
+        }
+        // scalar columns of block column kb
+        const int len = static_cast<int>(J.size()) * bs;
+        for (int cc = 0; cc < bs; cc++) {
+            const int col = kb * bs + cc;
+            out_len[col] = len;
+            if (len > out_stride)
+                return -1 - col;
+            for (int jj = 0; jj < len; jj++) {
+                out_idx[static_cast<size_t>(col) * out_stride + jj] = J[jj / bs] * bs + jj % bs;
+                out_val[static_cast<size_t>(col) * out_stride + jj] =
+                    X[cc * static_cast<size_t>(m) + jj];
+            }
+            out_res[col] = res;
+            out_steps[col] = steps;
+            out_info[col] = info;
+        }
+    }
+    return 0;
+}
+
 }  // extern "C"
