@@ -198,6 +198,31 @@ void mspai_free(mspai_handle* h);
  */
 int mspai_measure_fma_peak(int32_t device, int32_t fp64, double* gflops);
 
+/*
+ * Fixed-pattern setup that allocates nothing.  No counterpart in the
+ * reference (which allocates per call, src/Matrix.imp:178-283).
+ *
+ * For callers that cannot call cudaMalloc when they need the preconditioner:
+ * applications whose device memory is owned by their own pool or by another
+ * framework, and latency-critical paths that must not pay for cudaMalloc /
+ * cudaFree.  It runs the same column solver as mspai_setup with its scratch
+ * in a fixed 64 MiB array inside the library (held by every GPU that loads the
+ * library until the process exits) and calls no allocating routine.
+ *
+ * All of C, B (optional), P and the outputs are device arrays on the current
+ * device: values_out receives M's values at P's nonzeros (M has P's pattern),
+ * resnorm_out and status_out one entry per column.  Limits: ns = 0, bs = 1,
+ * at most 1,048,576 columns, at most 512 entries of C(:, J_k) and |J_k| <= 64
+ * per column; larger inputs are rejected with MSPAI_ERR_CAPACITY and a message
+ * in msg.  The first call on a device looks up the array's device address;
+ * make that call before any stream capture.  All calls share the array and it
+ * keeps the last call's contents: calls whose kernels overlap on the GPU race
+ * and must be serialised by the caller.  `stream` may be NULL (legacy stream).
+ */
+int mspai_setup_fixed_noalloc(const mspai_csc* C, const mspai_csc* B, const mspai_csc* P,
+                              const mspai_params* prm, double* values_out, double* resnorm_out,
+                              int32_t* status_out, void* stream, char* msg, int32_t msg_len);
+
 /* Library version string. */
 const char* mspai_version(void);
 

@@ -62,7 +62,7 @@ EXPORTED = [
     "mspai_adjoint", "mspai_last_error", "mspai_free", "mspai_version",
     "mspai_matrix_view", "mspai_matrix_free", "mspai_mm_read", "mspai_mm_write",
     "mspai_probing_assemble", "mspai_pattern_generate", "mspai_row_structure",
-    "mspai_measure_fma_peak",
+    "mspai_measure_fma_peak", "mspai_setup_fixed_noalloc",
 ]
 
 _lib = None
@@ -105,6 +105,10 @@ def load() -> ctypes.CDLL:
     lib.mspai_measure_fma_peak.argtypes = [ctypes.c_int32, ctypes.c_int32,
                                            ctypes.POINTER(ctypes.c_double)]
     lib.mspai_measure_fma_peak.restype = I
+    lib.mspai_setup_fixed_noalloc.argtypes = [P(mspai_csc), P(mspai_csc), P(mspai_csc),
+                                              P(mspai_params), V, V, V, V, ctypes.c_char_p,
+                                              ctypes.c_int32]
+    lib.mspai_setup_fixed_noalloc.restype = I
     lib.mspai_version.argtypes = []
     lib.mspai_version.restype = ctypes.c_char_p
     lib.mspai_mm_read.argtypes = [ctypes.c_char_p, P(mspai_matrix), ctypes.c_char_p,
