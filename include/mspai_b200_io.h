@@ -63,6 +63,16 @@ int mspai_probing_assemble(const mspai_csc* A, const mspai_csc* Ce, const mspai_
  */
 int mspai_pattern_generate(const mspai_csc* C, int32_t kind, mspai_matrix* P_out);
 
+/*
+ * Block start patterns for constant block size bs (n / bs block columns):
+ * kind 1 = diagonal blocks, kind 2 = the block pattern of C's first n rows
+ * (a block is present when any of its entries is stored), as the reference's
+ * Diagonal_Pattern / To_Pattern on the block matrix of
+ * Matrix::Convert_Block_Matrix (src/Matrix.imp:1280-1360).
+ */
+int mspai_block_pattern_generate(const mspai_csc* C, int32_t bs, int32_t kind,
+                                 mspai_matrix* P_out);
+
 /* CSR row structure of the first nrows_keep rows of C, as a CSC of C^T. */
 int mspai_row_structure(const mspai_csc* C, int32_t nrows_keep, mspai_matrix* R_out);
 

@@ -62,7 +62,7 @@ EXPORTED = [
     "mspai_adjoint", "mspai_last_error", "mspai_free", "mspai_version",
     "mspai_matrix_view", "mspai_matrix_free", "mspai_mm_read", "mspai_mm_write",
     "mspai_probing_assemble", "mspai_pattern_generate", "mspai_row_structure",
-    "mspai_measure_fma_peak", "mspai_setup_fixed_noalloc",
+    "mspai_measure_fma_peak", "mspai_setup_fixed_noalloc", "mspai_block_pattern_generate",
 ]
 
 _lib = None
@@ -125,6 +125,9 @@ def load() -> ctypes.CDLL:
     lib.mspai_probing_assemble.restype = I
     lib.mspai_pattern_generate.argtypes = [P(mspai_csc), ctypes.c_int32, P(mspai_matrix)]
     lib.mspai_pattern_generate.restype = I
+    lib.mspai_block_pattern_generate.argtypes = [P(mspai_csc), ctypes.c_int32, ctypes.c_int32,
+                                                 P(mspai_matrix)]
+    lib.mspai_block_pattern_generate.restype = I
     lib.mspai_row_structure.argtypes = [P(mspai_csc), ctypes.c_int32, P(mspai_matrix)]
     lib.mspai_row_structure.restype = I
     _lib = lib

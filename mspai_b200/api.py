@@ -327,6 +327,22 @@ def start_pattern(C: sp.spmatrix, kind: Union[int, str]) -> sp.csc_matrix:
         lib.mspai_matrix_free(ctypes.byref(m))
 
 
+def block_pattern(C: sp.spmatrix, bs: int, kind: Union[int, str]) -> sp.csc_matrix:
+    """Block start pattern (n/bs x n/bs): -1 / "diag" diagonal blocks, -2 / "A"
+    the block pattern of C's first n rows (mspai_block_pattern_generate)."""
+    k = {"diag": 1, -1: 1, 1: 1, "A": 2, -2: 2, 2: 2}[kind]
+    lib = _lib.load()
+    s = _Staged(C, False)
+    m = _lib.mspai_matrix()
+    rc = lib.mspai_block_pattern_generate(ctypes.byref(s.c), int(bs), k, ctypes.byref(m))
+    if rc != _lib.MSPAI_OK:
+        raise MspaiError(rc, "block pattern generation failed")
+    try:
+        return _owned_to_scipy(m)
+    finally:
+        lib.mspai_matrix_free(ctypes.byref(m))
+
+
 def mspai(A: sp.spmatrix, pattern: Union[int, str, sp.spmatrix] = -1,
           target: Optional[sp.spmatrix] = None, Ce: Optional[sp.spmatrix] = None,
           Be: Optional[sp.spmatrix] = None, UP: Optional[sp.spmatrix] = None,
@@ -340,7 +356,12 @@ def mspai(A: sp.spmatrix, pattern: Union[int, str, sp.spmatrix] = -1,
     Bin = B if opts.probing else None
     if target is not None:
         Bin = target
-    P = pattern if sp.issparse(pattern) else start_pattern(C, pattern)
+    if sp.issparse(pattern):
+        P = pattern
+    elif opts.bs > 1:
+        P = block_pattern(C, opts.bs, pattern)
+    else:
+        P = start_pattern(C, pattern)
     h = Handle(device)
     h.setup(C, P, B=Bin, UP=UP, options=opts)
     return h.result(), h

@@ -120,10 +120,11 @@ __device__ void adjoint_column(const G& g, const Problem& pb, const Caps& cap, S
         }
     }
     g.sync();
-    group_householder<double>(g, W, ld, mw, n, rhs);
+    group_householder<double>(g, W, ld, mw, n, 1);
     group_back_substitute<double>(g, W, ld, n, rhs, s.x);
     // r = b - C m on I
-    const double r2 = group_residual(g, pb, col, s.keys, s.I, s.rstart, s.ejj, s.ev, s.x, s.r, m);
+    const double r2 =
+        group_residual(g, pb, col, s.keys, s.I, s.rstart, s.ejj, s.ev, s.x, s.r, m, n, 1);
     // lambda = R^-1 R^-T gbar_k
     double gx = 0.0;
     if (io.gbar) {

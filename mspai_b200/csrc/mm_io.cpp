@@ -285,6 +285,35 @@ int mspai_pattern_generate(const mspai_csc* C, int32_t kind, mspai_matrix* P_out
     return triplets_to_csc(n, n, t, false, P_out);
 }
 
+int mspai_block_pattern_generate(const mspai_csc* C, int32_t bs, int32_t kind,
+                                 mspai_matrix* P_out)
+{
+    std::memset(P_out, 0, sizeof(*P_out));
+    if (!C || C->mem != MSPAI_MEM_HOST || bs < 1 || C->ncols % bs != 0)
+        return MSPAI_ERR_PARAM;
+    const int n = C->ncols, nb = n / bs;
+    std::vector<Triplet> t;
+    if (kind == 1) {
+        for (int c = 0; c < nb; c++)
+            t.push_back({c, c, 1.0});
+    }
+    else if (kind == 2) {
+        for (int c = 0; c < n; c++)
+            for (int64_t q = C->colptr[c]; q < C->colptr[c + 1]; q++) {
+                if (C->rowidx[q] >= n)
+                    break;
+                t.push_back({C->rowidx[q] / bs, c / bs, 1.0});
+            }
+    }
+    else {
+        return MSPAI_ERR_PARAM;
+    }
+    for (auto& x : t)
+        x.v = 0.0;  // duplicates are summed: keep a pattern
+    int rc = triplets_to_csc(nb, nb, t, false, P_out);
+    return rc;
+}
+
 int mspai_row_structure(const mspai_csc* C, int32_t nrows_keep, mspai_matrix* R_out)
 {
     std::memset(R_out, 0, sizeof(*R_out));

@@ -241,6 +241,7 @@ extern "C" int mspai_setup_fixed_noalloc(const mspai_csc* C, const mspai_csc* B,
         pb.bidx = B->rowidx;
         pb.bval = B->values;
     }
+    pb.bs = 1;
     pb.ep = prm->ep;
     pb.mn = prm->mn;
     pb.ns = 0;
@@ -254,6 +255,8 @@ extern "C" int mspai_setup_fixed_noalloc(const mspai_csc* C, const mspai_csc* B,
     cap.mwmax = cap.emax / 2 + cap.nmax;
     cap.cmax = 0;
     cap.lcand = 0;
+    cap.nrhs = 1;
+    cap.nbmap = 0;
     if (n > kNoAllocMaxColumns)
         return fail(MSPAI_ERR_CAPACITY, "more columns than the no-allocation limit (1048576)");
     Output out{};

@@ -92,7 +92,8 @@ struct mspai_handle {
     mspai_stats stats{};
     mspai_params last_params{};
     int64_t launches = 0;
-    size_t smem_budget = 200 * 1024;  // shared-memory area of the CTA solver
+    int nprob = 0;  // problem columns of the last setup (n / bs)
+    size_t smem_budget = 48 * 1024;  // shared-memory area of each CTA solver (4 per SM)
 };
 
 static int set_err(mspai_handle* h, int code, const char* fmt, ...)
@@ -278,18 +279,24 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     int rc = mspai_validate_params(prm, msg, sizeof(msg));
     if (rc != MSPAI_OK)
         return set_err(h, rc, "%s", msg);
-    if (prm->bs != 1)
-        return set_err(h, MSPAI_ERR_PARAM, "block SPAI (-bs %d) is served by mspai_setup_block",
-                       prm->bs);
     const int n = C->ncols;
+    const int bs = prm->bs;
+    if (bs > 4)
+        return set_err(h, MSPAI_ERR_PARAM, "block size %d not supported (1..4)", bs);
+    if (n % bs != 0)
+        return set_err(h, MSPAI_ERR_INPUT,
+                       "block size %d does not divide the %d columns (constant blocks only)", bs,
+                       n);
+    const int nprob = n / bs;  // problem columns: scalar columns or block columns
     if ((rc = check_csc(h, C, "C", true)) != MSPAI_OK)
         return rc;
     if ((rc = check_csc(h, P, "P", false)) != MSPAI_OK)
         return rc;
     if (C->nrows < n)
         return set_err(h, MSPAI_ERR_INPUT, "C has fewer rows (%d) than columns (%d)", C->nrows, n);
-    if (P->ncols != n || P->nrows != n)
-        return set_err(h, MSPAI_ERR_INPUT, "pattern must be %d x %d", n, n);
+    if (P->ncols != nprob || P->nrows != nprob)
+        return set_err(h, MSPAI_ERR_INPUT, "%spattern must be %d x %d", bs > 1 ? "block " : "",
+                       nprob, nprob);
     if (B) {
         if ((rc = check_csc(h, B, "B", true)) != MSPAI_OK)
             return rc;
@@ -322,7 +329,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     CUDA_TRY(h, stage(h->cptr, C->colptr, n + 1, C->mem, st, &pb.cptr));
     CUDA_TRY(h, stage(h->cidx, C->rowidx, C->nnz, C->mem, st, &pb.cidx));
     CUDA_TRY(h, stage(h->cval, C->values, C->nnz, C->mem, st, &pb.cval));
-    CUDA_TRY(h, stage(h->pptr, P->colptr, n + 1, P->mem, st, &pb.pptr));
+    CUDA_TRY(h, stage(h->pptr, P->colptr, nprob + 1, P->mem, st, &pb.pptr));
     CUDA_TRY(h, stage(h->pidx, P->rowidx, P->nnz, P->mem, st, &pb.pidx));
     if (B) {
         CUDA_TRY(h, stage(h->bptr, B->colptr, n + 1, B->mem, st, &pb.bptr));
@@ -361,6 +368,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
         for (size_t i = 0; i + 1 < rp.size(); i++)
             max_row_nnz = std::max<int>(max_row_nnz, static_cast<int>(rp[i + 1] - rp[i]));
     }
+    pb.bs = bs;
     pb.ep = prm->ep;
     pb.mn = prm->mn;
     pb.ns = adaptive ? prm->ns : 0;
@@ -391,15 +399,18 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     CUDA_TRY(h, cudaMemsetAsync(h->work.p, 0, sizeof(double) * 3 * std::max(n, 1), st));
     CUDA_TRY(h, h->scan_tmp.ensure(sizeof(int64_t) * ((n + 1023) / 1024 + 2)));
     int64_t cap_total = P->nnz;
-    if (adaptive) {
+    const bool compact = adaptive || bs > 1;  // M's pattern differs from P's
+    h->fixed_pattern = !compact;
+    if (compact) {
         CUDA_TRY(h, h->cap_len.ensure(sizeof(int32_t) * std::max(n, 1)));
         CUDA_TRY(h, h->cap_ptr.ensure(sizeof(int64_t) * (n + 1)));
         h->launches++;
-    CUDA_TRY(h, mspai::launch_capacity_len(pb.pptr, n, grow_n, h->cap_len.as<int32_t>(), st));
+        CUDA_TRY(h, mspai::launch_capacity_len(pb.pptr, n, bs, grow_n, h->cap_len.as<int32_t>(),
+                                               st));
         h->launches += 4;
         CUDA_TRY(h, mspai::launch_scan_lengths(h->cap_len.as<int32_t>(), n, h->cap_ptr.as<int64_t>(),
                                                h->scan_tmp.as<int64_t>(), st));
-        cap_total = P->nnz + static_cast<int64_t>(grow_n) * n;
+        cap_total = (P->nnz + static_cast<int64_t>(grow_n) * nprob) * bs * bs;
         CUDA_TRY(h, h->oidx.ensure(sizeof(int32_t) * std::max<int64_t>(cap_total, 1)));
         out.optr = h->cap_ptr.as<int64_t>();
         out.oidx = h->oidx.as<int32_t>();
@@ -419,25 +430,26 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     out.work = h->work.as<double>();
 
     // ---- plan and bucket
-    CUDA_TRY(h, h->E.ensure(sizeof(int32_t) * std::max(n, 1)));
-    CUDA_TRY(h, h->nk.ensure(sizeof(int32_t) * std::max(n, 1)));
-    CUDA_TRY(h, h->lists.ensure(sizeof(int32_t) * static_cast<size_t>(kBuckets) * std::max(n, 1)));
+    CUDA_TRY(h, h->E.ensure(sizeof(int32_t) * std::max(nprob, 1)));
+    CUDA_TRY(h, h->nk.ensure(sizeof(int32_t) * std::max(nprob, 1)));
+    CUDA_TRY(h, h->lists.ensure(sizeof(int32_t) * static_cast<size_t>(kBuckets) *
+                                std::max(nprob, 1)));
     h->launches++;
-    CUDA_TRY(h, mspai::launch_plan(pb.cptr, pb.pptr, pb.pidx, n, h->E.as<int32_t>(),
+    CUDA_TRY(h, mspai::launch_plan(pb.cptr, pb.pptr, pb.pidx, nprob, bs, h->E.as<int32_t>(),
                                    h->nk.as<int32_t>(), st));
     CUDA_TRY(h, cudaStreamSynchronize(st));  // max_col_nnz is on the host now
     BucketRule rule{};
     rule.single_bucket = prm->batched ? -1 : 2;
-    rule.allow_warp = adaptive ? 0 : 1;
+    rule.allow_warp = (adaptive || bs > 1) ? 0 : 1;
     rule.warp_emax = 64;
     rule.warp_nmax = 16;
     rule.smem_w_bytes = 96 * 1024;
     rule.elem_bytes = elem;
-    rule.grow_n = grow_n;
-    rule.grow_e = adaptive ? grow_n * max_col_nnz : 0;
+    rule.grow_n = grow_n * bs;
+    rule.grow_e = adaptive ? grow_n * bs * max_col_nnz : 0;
     CUDA_TRY(h, cudaMemsetAsync(dcnt, 0, sizeof(int32_t) * 16, st));
     h->launches++;
-    CUDA_TRY(h, mspai::launch_bucket(h->E.as<int32_t>(), h->nk.as<int32_t>(), n, rule, dcnt,
+    CUDA_TRY(h, mspai::launch_bucket(h->E.as<int32_t>(), h->nk.as<int32_t>(), nprob, rule, dcnt,
                                      dcnt + 4, dcnt + 8, h->lists.as<int32_t>(), st));
     int32_t hc[16];
     CUDA_TRY(h, cudaMemcpyAsync(hc, dcnt, sizeof(hc), cudaMemcpyDeviceToHost, st));
@@ -457,12 +469,19 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
         cap.nmax = std::max(1, hc[8 + b]);
         cap.lsort = mspai::next_pow2(cap.emax);
         cap.mwmax = cap.emax / 2 + cap.nmax;
-        cap.cmax = adaptive ? (cap.emax + 1) * std::max(1, max_row_nnz) : 0;
+        cap.nrhs = bs;
+        // unique candidates: at most the problem columns, at most the row
+        // structure entries of L's rows
+        cap.cmax = adaptive ? static_cast<int>(std::min<int64_t>(
+                                  nprob, static_cast<int64_t>(cap.emax + 1) * bs *
+                                             std::max(1, max_row_nnz)))
+                            : 0;
         cap.lcand = adaptive ? mspai::next_pow2(cap.cmax) : 0;
+        cap.nbmap = adaptive ? (nprob + 31) / 32 : 0;
         if (static_cast<int64_t>(cap.emax) >= mspai::kMaxEntries)
             return set_err(h, MSPAI_ERR_CAPACITY, "a column touches %d entries of C (max %d)",
                            cap.emax, mspai::kMaxEntries - 1);
-        int32_t* list = h->lists.as<int32_t>() + static_cast<size_t>(b) * n;
+        int32_t* list = h->lists.as<int32_t>() + static_cast<size_t>(b) * nprob;
         int32_t* counter = dcnt + 12 + b;
         CUDA_TRY(h, cudaMemsetAsync(counter, 0, sizeof(int32_t), st));
         CUDA_TRY(h, cudaEventRecord(h->evb[2 * b], st));
@@ -485,6 +504,8 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
                 wsm = 0;  // the plain path keeps W in global memory, unblocked
             const size_t need = mspai::cta_scratch_needed(elem, cap, count);
             CUDA_TRY(h, h->scratch.ensure(need));
+            if (adaptive)  // the candidate bit vectors of the slots start cleared
+                CUDA_TRY(h, cudaMemsetAsync(h->scratch.p, 0, need, st));
             h->launches++;
             CUDA_TRY(h, mspai::launch_cta_solve(elem, wsm, prm->batched != 0, pb, cap, out, list,
                                                 count, counter,
@@ -495,7 +516,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     }
 
     // ---- assemble M
-    if (adaptive) {
+    if (compact) {
         CUDA_TRY(h, h->mptr.ensure(sizeof(int64_t) * (n + 1)));
         h->launches += 4;
         CUDA_TRY(h, mspai::launch_scan_lengths(out.olen, n, h->mptr.as<int64_t>(),
@@ -549,6 +570,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
         }
     }
     h->stats.columns = n;
+    h->nprob = nprob;
     h->stats.nnz_m = h->nnz_m;
     h->stats.kernel_launches = h->launches;
     h->last_params = *prm;
@@ -623,13 +645,14 @@ int mspai_get_stats(mspai_handle* h, mspai_stats* s)
     // algorithmic flops per bucket kernel (columns listed per bucket)
     for (int b = 0; b < 4; b++)
         h->stats.bucket_flops[b] = 0.0;
-    if (h->n > 0 && h->lists.p) {
-        std::vector<int32_t> lists(static_cast<size_t>(kBuckets) * h->n);
+    if (h->nprob > 0 && h->lists.p) {
+        std::vector<int32_t> lists(static_cast<size_t>(kBuckets) * h->nprob);
         CUDA_TRY(h, cudaMemcpy(lists.data(), h->lists.p, sizeof(int32_t) * lists.size(),
                                cudaMemcpyDeviceToHost));
         for (int b = 0; b < kBuckets; b++)
             for (int64_t t = 0; t < h->stats.bucket_columns[b]; t++)
-                h->stats.bucket_flops[b] += work[3 * static_cast<size_t>(lists[b * static_cast<size_t>(h->n) + t])];
+                h->stats.bucket_flops[b] +=
+                    work[3 * static_cast<size_t>(lists[b * static_cast<size_t>(h->nprob) + t])];
     }
     for (int c = 0; c < h->n; c++) {
         fl += work[3 * c];
@@ -683,6 +706,7 @@ extern "C" int mspai_adjoint(mspai_handle* h, const mspai_csc* C, const mspai_cs
     }
     pb.pptr = h->res_ptr;
     pb.pidx = h->res_idx;
+    pb.bs = 1;
     mspai::AdjointIO io{};
     io.mptr = h->res_ptr;
     DevBuf gbuf, dcbuf, dbbuf, lossbuf, cnt;
@@ -715,7 +739,7 @@ extern "C" int mspai_adjoint(mspai_handle* h, const mspai_csc* C, const mspai_cs
     CUDA_TRY(h, h->nk.ensure(sizeof(int32_t) * std::max(n, 1)));
     CUDA_TRY(h, h->lists.ensure(sizeof(int32_t) * 3 * static_cast<size_t>(std::max(n, 1))));
     h->launches++;
-    CUDA_TRY(h, mspai::launch_plan(pb.cptr, pb.pptr, pb.pidx, n, h->E.as<int32_t>(),
+    CUDA_TRY(h, mspai::launch_plan(pb.cptr, pb.pptr, pb.pidx, n, 1, h->E.as<int32_t>(),
                                    h->nk.as<int32_t>(), st));
     BucketRule rule{};
     rule.single_bucket = 0;
@@ -733,6 +757,8 @@ extern "C" int mspai_adjoint(mspai_handle* h, const mspai_csc* C, const mspai_cs
     cap.mwmax = cap.emax / 2 + cap.nmax;
     cap.cmax = cap.emax;  // q = C lambda is kept in the rho[] area
     cap.lcand = 0;
+    cap.nrhs = 1;
+    cap.nbmap = 0;
     const bool warp = cap.emax <= 64 && cap.nmax <= 16;
     const size_t need = mspai::adjoint_scratch_bytes(cap, n, warp);
     CUDA_TRY(h, h->scratch.ensure(need));

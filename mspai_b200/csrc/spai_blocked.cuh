@@ -20,7 +20,9 @@
 namespace mspai {
 
 constexpr int kPanel = 16;     // panel width
-constexpr int kTileCols = 4;   // trailing columns per warp tile
+constexpr int kTileCols = 2;   // trailing columns per warp tile
+constexpr int kTileVals = kTileCols * kPanel;  // partial sums per lane
+constexpr int kPerLane = kTileVals / 32;        // reduced sums per lane
 
 // Shared-memory scratch of the blocked routines (besides the W/panel area).
 template <class T>
@@ -132,27 +134,27 @@ __device__ void panel_tfactor(const G& g, const T* P, int ldp, int mp, int nb,
 }
 
 // Trailing update of `ncols` columns starting at W2 (ld ldw, rows aligned with
-// the panel's rows) plus the right-hand side `rhs2` (treated as column ncols):
+// the panel's rows; the right-hand sides are the last columns):
 //   X <- X - V (T^T (V^T X)).
 template <class T, class G>
 __device__ void trailing_update(const G& g, const T* P, int ldp, int mp, int nb,
-                                const BlockedScratch<T>* bs, T* W2, int ldw, int ncols, T* rhs2)
+                                const BlockedScratch<T>* bs, T* W2, int ldw, int ncols)
 {
     const int lane = g.lane();
-    const int total = ncols + 1;
+    const int total = ncols;
     for (int cb = g.warp() * kTileCols; cb < total; cb += G::kWarps * kTileCols) {
         T* col[kTileCols];
 #pragma unroll
         for (int c = 0; c < kTileCols; c++) {
             const int cc = cb + c;
-            col[c] = (cc < ncols) ? W2 + static_cast<size_t>(cc) * ldw : (cc == ncols ? rhs2 : nullptr);
+            col[c] = (cc < ncols) ? W2 + static_cast<size_t>(cc) * ldw : nullptr;
         }
         // Y = V^T X (partial sums per lane over its rows).  Rows are taken four
         // at a time so that 16 independent loads of X are in flight per lane
         // (X may be in global memory).
-        T acc[kTileCols * kPanel];
+        T acc[kTileVals];
 #pragma unroll
-        for (int t = 0; t < kTileCols * kPanel; t++)
+        for (int t = 0; t < kTileVals; t++)
             acc[t] = T(0);
         constexpr int kRows = 4;
         int r0 = lane;
@@ -188,14 +190,15 @@ __device__ void trailing_update(const G& g, const T* P, int ldp, int mp, int nb,
                     acc[c * kPanel + i] += v * x[c];
             }
         }
-        // warp reduce-scatter: lane l ends with the sums of entries 2l, 2l+1
+        // warp reduce-scatter: lane l ends with the sums of entries
+        // kPerLane * l .. kPerLane * l + kPerLane - 1
 #pragma unroll
         for (int level = 0; level < 5; level++) {
-            const int half = (kTileCols * kPanel) >> (level + 1);
+            const int half = kTileVals >> (level + 1);
             const int bit = 16 >> level;
             const bool upper = (lane & bit) != 0;
 #pragma unroll
-            for (int t = 0; t < 32; t++) {
+            for (int t = 0; t < kTileVals / 2; t++) {
                 if (t < half) {
                     const T mine = upper ? acc[half + t] : acc[t];
                     const T other = upper ? acc[t] : acc[half + t];
@@ -203,29 +206,31 @@ __device__ void trailing_update(const G& g, const T* P, int ldp, int mp, int nb,
                 }
             }
         }
-        // Y entries 2*lane, 2*lane+1 -> Z = T^T Y via shared exchange of Y
-        __shared__ T ybuf_all[G::kWarps][kTileCols * kPanel];  // one row per warp
+        // Y -> Z = T^T Y via a shared exchange of Y (one row per warp)
+        __shared__ T ybuf_all[G::kWarps][kTileVals];
         T* ybuf = ybuf_all[g.warp()];
-        ybuf[2 * lane] = acc[0];
-        ybuf[2 * lane + 1] = acc[1];
-        __syncwarp();
-        T z2[2];
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int idx = 2 * lane + h;
+        for (int h = 0; h < kPerLane; h++)
+            ybuf[kPerLane * lane + h] = acc[h];
+        __syncwarp();
+        T zl[kPerLane];
+#pragma unroll
+        for (int h = 0; h < kPerLane; h++) {
+            const int idx = kPerLane * lane + h;
             const int c = idx / kPanel, i = idx % kPanel;
             T z = 0;
             for (int j = 0; j <= i && j < nb; j++)
                 z += bs->tmat[j + i * kPanel] * ybuf[c * kPanel + j];
-            z2[h] = (i < nb) ? z : T(0);
+            zl[h] = (i < nb) ? z : T(0);
         }
         __syncwarp();
-        ybuf[2 * lane] = z2[0];
-        ybuf[2 * lane + 1] = z2[1];
-        __syncwarp();
-        T zr[kTileCols * kPanel];
 #pragma unroll
-        for (int t = 0; t < kTileCols * kPanel; t++)
+        for (int h = 0; h < kPerLane; h++)
+            ybuf[kPerLane * lane + h] = zl[h];
+        __syncwarp();
+        T zr[kTileVals];
+#pragma unroll
+        for (int t = 0; t < kTileVals; t++)
             zr[t] = ybuf[t];
         // X -= V Z (four rows per lane at a time: loads first, then stores)
         int r1 = lane;
@@ -275,11 +280,12 @@ __device__ void trailing_update(const G& g, const T* P, int ldp, int mp, int nb,
     }
 }
 
-// Blocked Householder QR of W (mw x n, ld) applied to rhs.  `region` is a
-// shared-memory area of at least mw * kPanel elements used to stage panels
-// when W is not itself in shared memory (w_in_smem == false).
+// Blocked Householder QR of W (mw x n, ld) applied to the nrhs right-hand
+// sides stored as the next columns of W.  `region` is a shared-memory area of
+// at least mw * kPanel elements used to stage panels when W is not itself in
+// shared memory (w_in_smem == false).
 template <class T, class G>
-__device__ void group_householder_blocked(const G& g, T* W, int ld, int mw, int n, T* rhs,
+__device__ void group_householder_blocked(const G& g, T* W, int ld, int mw, int n, int nrhs,
                                           bool w_in_smem, T* region, BlockedScratch<T>* bs)
 {
     const int kmax = min(mw, n);
@@ -313,7 +319,7 @@ __device__ void group_householder_blocked(const G& g, T* W, int ld, int mw, int 
             }
         }
         trailing_update<T>(g, P, ldp, mp, nb, bs, W + static_cast<size_t>(c0 + nb) * ld + c0, ld,
-                           n - c0 - nb, rhs + c0);
+                           n - c0 - nb + nrhs);
         g.sync();
     }
 }

@@ -53,9 +53,10 @@ __device__ __forceinline__ double tsqrt<double>(double v)
 
 // Shared scratch a group needs for reductions and broadcasts.
 struct GroupScratch {
-    double red[32];
+    double red[32];  // reductions (two halves of 16, see CtaGroup::sum)
     double d[4];
     int i[8];
+    int scan[32];    // per-warp totals of group_exclusive_scan
 };
 
 struct WarpGroup {
@@ -79,6 +80,10 @@ struct CtaGroup {
     GroupScratch* sc;
     static constexpr int kSize = NT;
     static constexpr int kWarps = NT / 32;
+    // reductions alternate between two halves of sc->red so that one barrier
+    // per reduction suffices (a warp cannot overwrite a half that a slower warp
+    // is still reading: the next reduction's barrier lies in between)
+    mutable int parity = 0;
     __device__ __forceinline__ int rank() const { return threadIdx.x; }
     __device__ __forceinline__ int warp() const { return threadIdx.x >> 5; }
     __device__ __forceinline__ int lane() const { return threadIdx.x & 31; }
@@ -86,20 +91,17 @@ struct CtaGroup {
     template <class T>
     __device__ __forceinline__ T sum(T v) const
     {
+        static_assert(kWarps <= 16, "two halves of 16 partial sums");
         v = warp_sum(v);
+        double* half = sc->red + 16 * parity;
+        parity ^= 1;
         if (lane() == 0)
-            sc->red[warp()] = static_cast<double>(v);
+            half[warp()] = static_cast<double>(v);
         __syncthreads();
         double t = 0.0;
-        if (threadIdx.x < 32) {
-            t = threadIdx.x < kWarps ? sc->red[threadIdx.x] : 0.0;
-            t = warp_sum(t);
-            if (threadIdx.x == 0)
-                sc->d[3] = t;
-        }
-        __syncthreads();
-        t = sc->d[3];
-        __syncthreads();
+#pragma unroll
+        for (int w = 0; w < kWarps; w++)
+            t += half[w];
         return static_cast<T>(t);
     }
     __device__ __forceinline__ int bcast(int v) const
@@ -133,7 +135,7 @@ __device__ int group_exclusive_scan(const G& g, int* a, int len)
         if (lane >= o)
             v += t;
     }
-    int* part = reinterpret_cast<int*>(g.sc->red);
+    int* part = g.sc->scan;
     if constexpr (G::kWarps > 1) {
         if (lane == 31)
             part[g.warp()] = v;

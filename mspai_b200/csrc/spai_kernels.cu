@@ -36,24 +36,25 @@ extern "C" int mspai_profile_phase_cycles(unsigned long long* out, int reset)
 
 // ------------------------------------------------------------------ planning
 __global__ void plan_kernel(const int64_t* __restrict__ cptr, const int64_t* __restrict__ pptr,
-                            const int32_t* __restrict__ pidx, int n, int32_t* __restrict__ E,
-                            int32_t* __restrict__ nk)
+                            const int32_t* __restrict__ pidx, int nprob, int bs,
+                            int32_t* __restrict__ E, int32_t* __restrict__ nk)
 {
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int col = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; col < n; col += warps) {
+    for (int col = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; col < nprob; col += warps) {
         const int64_t a = pptr[col], b = pptr[col + 1];
         int64_t e = 0;
         for (int64_t p = a + lane; p < b; p += 32) {
             const int j = pidx[p];
-            e += cptr[j + 1] - cptr[j];
+            for (int c = 0; c < bs; c++)
+                e += cptr[bs * j + c + 1] - cptr[bs * j + c];
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1)
             e += __shfl_xor_sync(0xffffffffu, e, o);
         if (lane == 0) {
             E[col] = static_cast<int32_t>(e > 0x7fffffff ? 0x7fffffff : e);
-            nk[col] = static_cast<int32_t>(b - a);
+            nk[col] = static_cast<int32_t>((b - a) * bs);
         }
     }
 }
@@ -110,8 +111,10 @@ __global__ void __launch_bounds__(kWarpKernelThreads)
     }
 }
 
+// 128-thread CTAs are bounded to 128 registers per thread so that four columns
+// are solved concurrently on every SM.
 template <class T, int NT>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, NT == 128 ? 4 : 1)
     cta_solve_kernel(Problem pb, Caps cap, Output out, const int32_t* __restrict__ list, int count,
                      int32_t* __restrict__ counter, char* __restrict__ scratch, size_t slot_bytes,
                      int wfast_elems, int blocked)
@@ -203,11 +206,14 @@ __global__ void finish_ptr_kernel(int64_t* __restrict__ ptr, int n, const int32_
         ptr[n] = (n > 0) ? ptr[n - 1] + len[n - 1] : 0;
 }
 
-__global__ void capacity_len_kernel(const int64_t* __restrict__ pptr, int n, int grow,
+// capacity of scalar column sc: bs * (|P(:, sc / bs)| + grow) entries
+__global__ void capacity_len_kernel(const int64_t* __restrict__ pptr, int n, int bs, int grow,
                                     int32_t* __restrict__ len)
 {
-    for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < n; col += gridDim.x * blockDim.x)
-        len[col] = static_cast<int32_t>(pptr[col + 1] - pptr[col]) + grow;
+    for (int sc = blockIdx.x * blockDim.x + threadIdx.x; sc < n; sc += gridDim.x * blockDim.x) {
+        const int kb = sc / bs;
+        len[sc] = static_cast<int32_t>((pptr[kb + 1] - pptr[kb] + grow) * bs);
+    }
 }
 
 __global__ void max_len_kernel(const int64_t* __restrict__ ptr, int n, int32_t* __restrict__ out)
@@ -238,15 +244,15 @@ int num_sms()
 }
 }  // namespace
 
-cudaError_t launch_plan(const int64_t* cptr, const int64_t* pptr, const int32_t* pidx, int n,
-                        int32_t* E, int32_t* nk, cudaStream_t st)
+cudaError_t launch_plan(const int64_t* cptr, const int64_t* pptr, const int32_t* pidx, int nprob,
+                        int bs, int32_t* E, int32_t* nk, cudaStream_t st)
 {
-    if (n <= 0)
+    if (nprob <= 0)
         return cudaSuccess;
     const int threads = 256;
-    int blocks = (n + 7) / 8;
+    int blocks = (nprob + 7) / 8;
     blocks = std::min(blocks, num_sms() * 16);
-    plan_kernel<<<blocks, threads, 0, st>>>(cptr, pptr, pidx, n, E, nk);
+    plan_kernel<<<blocks, threads, 0, st>>>(cptr, pptr, pidx, nprob, bs, E, nk);
     return cudaGetLastError();
 }
 
@@ -277,7 +283,7 @@ size_t cta_slot_bytes(const Caps& cap, int elem_bytes, bool w_smem)
 
 size_t w_bytes(const Caps& cap, int elem_bytes)
 {
-    return (static_cast<size_t>(cap.mwmax) * cap.nmax + cap.mwmax) * elem_bytes;
+    return static_cast<size_t>(cap.mwmax) * (cap.nmax + std::max(1, cap.nrhs)) * elem_bytes;
 }
 
 template <class T>
@@ -354,14 +360,11 @@ cudaError_t launch_cta_solve(int elem_bytes, size_t smem_w_bytes, bool blocked,
                              size_t scratch_bytes, cudaStream_t st, int* grid_out)
 {
     if (elem_bytes == 4)
-        return launch_cta_t<float, 256>(pb, cap, out, list, count, counter, scratch,
+        return launch_cta_t<float, 128>(pb, cap, out, list, count, counter, scratch,
                                         scratch_bytes, smem_w_bytes, blocked ? 1 : 0, st,
                                         grid_out);
-    if (blocked)
-        return launch_cta_t<double, 256>(pb, cap, out, list, count, counter, scratch,
-                                         scratch_bytes, smem_w_bytes, 1, st, grid_out);
     return launch_cta_t<double, 128>(pb, cap, out, list, count, counter, scratch, scratch_bytes,
-                                     smem_w_bytes, 0, st, grid_out);
+                                     smem_w_bytes, blocked ? 1 : 0, st, grid_out);
 }
 
 size_t cta_scratch_needed(int elem_bytes, const Caps& cap, int count)
@@ -387,12 +390,13 @@ cudaError_t launch_scan_lengths(const int32_t* len, int n, int64_t* ptr, int64_t
     return cudaGetLastError();
 }
 
-cudaError_t launch_capacity_len(const int64_t* pptr, int n, int grow, int32_t* len, cudaStream_t st)
+cudaError_t launch_capacity_len(const int64_t* pptr, int n, int bs, int grow, int32_t* len,
+                                cudaStream_t st)
 {
     if (n <= 0)
         return cudaSuccess;
     int blocks = std::min((n + 255) / 256, num_sms() * 8);
-    capacity_len_kernel<<<blocks, 256, 0, st>>>(pptr, n, grow, len);
+    capacity_len_kernel<<<blocks, 256, 0, st>>>(pptr, n, bs, grow, len);
     return cudaGetLastError();
 }
 

@@ -25,8 +25,10 @@ struct BucketRule {
     int grow_e;            // mn * ns * max column nnz of C
 };
 
-cudaError_t launch_plan(const int64_t* cptr, const int64_t* pptr, const int32_t* pidx, int n,
-                        int32_t* E, int32_t* nk, cudaStream_t st);
+// E[k] = entries of C in the (scalar) columns of problem column k, nk[k] =
+// its scalar pattern size (block pattern entries * bs)
+cudaError_t launch_plan(const int64_t* cptr, const int64_t* pptr, const int32_t* pidx, int nprob,
+                        int bs, int32_t* E, int32_t* nk, cudaStream_t st);
 cudaError_t launch_bucket(const int32_t* E, const int32_t* nk, int n, const BucketRule& rule,
                           int32_t* counts, int32_t* maxE, int32_t* maxN, int32_t* lists,
                           cudaStream_t st);
@@ -46,7 +48,7 @@ cudaError_t launch_cta_solve(int elem_bytes, size_t smem_w_bytes, bool blocked,
                              size_t scratch_bytes, cudaStream_t st, int* grid_out);
 cudaError_t launch_scan_lengths(const int32_t* len, int n, int64_t* ptr, int64_t* tmp,
                                 cudaStream_t st);
-cudaError_t launch_capacity_len(const int64_t* pptr, int n, int grow, int32_t* len,
+cudaError_t launch_capacity_len(const int64_t* pptr, int n, int bs, int grow, int32_t* len,
                                 cudaStream_t st);
 cudaError_t launch_compact(const int64_t* cap_ptr, const int32_t* cidx, const double* cval,
                            const int64_t* out_ptr, int32_t* oidx, double* oval, int n,

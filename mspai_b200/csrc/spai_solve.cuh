@@ -71,6 +71,7 @@ struct Problem {
     const int32_t* upidx;
     double ep;
     int mn, ns, um, refine;
+    int bs;                                  // block size (1: scalar SPAI)
 };
 
 // Results.  Column k's indices/values go to [optr[k], optr[k+1]).
@@ -95,6 +96,8 @@ struct Caps {
     int mwmax;     // rows of the folded matrix
     int cmax;      // candidate entries (row structure of L)
     int lcand;     // next_pow2(cmax)
+    int nrhs;      // right-hand sides (the block size)
+    int nbmap;     // words of the candidate bit vector (adaptive; 0 otherwise)
 };
 
 // Pointers of one problem slot's workspace.
@@ -120,6 +123,7 @@ struct Slot {
     double* gv;        // nmax  refinement right-hand side / correction
     int32_t* cand;     // lcand candidate column indices (adaptive)
     int32_t* ctmp;     // cmax + 1 candidate flags / scan
+    uint32_t* bmap;    // nbmap words: bit vector over problem columns (adaptive)
     double* rho;       // cmax
 };
 
@@ -133,7 +137,7 @@ __host__ __device__ inline size_t align_up(size_t v, size_t a)
 template <class T>
 struct SlotLayout {
     size_t o_J, o_off, o_ejj, o_ev, o_pos, o_keys, o_I, o_rstart, o_tmp, o_r, o_W, o_rhs, o_x,
-        o_gv, o_cand, o_ctmp, o_rho, bytes;
+        o_gv, o_cand, o_ctmp, o_rho, o_bmap, bytes;
     __host__ __device__ SlotLayout(const Caps& c, bool w_external)
     {
         size_t o = 0;
@@ -144,26 +148,28 @@ struct SlotLayout {
             return at;
         };
         o_keys = take(sizeof(uint64_t) * c.lsort);
+        const int nr = c.nrhs > 0 ? c.nrhs : 1;
         o_ev = take(sizeof(double) * c.emax);
-        o_r = take(sizeof(double) * c.emax);
-        o_x = take(sizeof(double) * c.nmax);
-        o_gv = take(sizeof(double) * c.nmax);
+        o_r = take(sizeof(double) * static_cast<size_t>(c.emax) * nr);
+        o_x = take(sizeof(double) * static_cast<size_t>(c.nmax) * nr);
+        o_gv = take(sizeof(double) * static_cast<size_t>(c.nmax) * nr);
         o_rho = take(sizeof(double) * (c.cmax > 0 ? c.cmax : 1));
         o_J = take(sizeof(int32_t) * c.nmax);
         o_off = take(sizeof(int32_t) * (c.nmax + 1));
         o_ejj = take(sizeof(int32_t) * c.emax);
-        o_pos = take(sizeof(int32_t) * c.emax);
+        o_pos = take(sizeof(int32_t) * (c.emax + 1));
         o_I = take(sizeof(int32_t) * c.emax);
         o_rstart = take(sizeof(int32_t) * (c.emax + 1));
         o_tmp = take(sizeof(int32_t) * (c.emax + 1));
         o_cand = take(sizeof(int32_t) * (c.lcand > 0 ? c.lcand : 1));
         o_ctmp = take(sizeof(int32_t) * (c.cmax + 1));
+        o_bmap = take(sizeof(uint32_t) * (c.nbmap > 0 ? c.nbmap : 1));
         if (w_external) {
             o_W = o_rhs = 0;
         }
         else {
             o_W = take(sizeof(T) * static_cast<size_t>(c.mwmax) * c.nmax);
-            o_rhs = take(sizeof(T) * c.mwmax);
+            o_rhs = take(sizeof(T) * static_cast<size_t>(c.mwmax) * nr);
         }
         bytes = align_up<T>(o, 128);
     }
@@ -184,6 +190,7 @@ struct SlotLayout {
         s.gv = reinterpret_cast<double*>(base + o_gv);
         s.cand = reinterpret_cast<int32_t*>(base + o_cand);
         s.ctmp = reinterpret_cast<int32_t*>(base + o_ctmp);
+        s.bmap = reinterpret_cast<uint32_t*>(base + o_bmap);
         s.rho = reinterpret_cast<double*>(base + o_rho);
         if (w_ext) {
             s.W = w_ext;
@@ -231,12 +238,13 @@ __device__ __forceinline__ int lower_bound_i32(const int32_t* a, int len, int v)
     return lo;
 }
 
-// Householder QR of W (mw x n, ld = mw) applied to rhs; R overwrites the upper
-// triangle.  Reflectors follow LAPACK's dlarfg convention: beta = -sign(alpha)
-// * ||(alpha, x)||, tau = (beta - alpha) / beta, v = x / (alpha - beta), and
-// tau = 0 (H = I) when x = 0.
+// Householder QR of W (mw x n, ld = mw) applied to the nrhs right-hand sides
+// stored as columns n .. n + nrhs - 1 of W (same leading dimension); R
+// overwrites the upper triangle.  Reflectors follow LAPACK's dlarfg
+// convention: beta = -sign(alpha) * ||(alpha, x)||, tau = (beta - alpha) /
+// beta, v = x / (alpha - beta), and tau = 0 (H = I) when x = 0.
 template <class T, class G>
-__device__ void group_householder(const G& g, T* W, int ld, int mw, int n, T* rhs)
+__device__ void group_householder(const G& g, T* W, int ld, int mw, int n, int nrhs)
 {
     const int kmax = min(mw, n);
     const int lane = g.lane();
@@ -258,9 +266,9 @@ __device__ void group_householder(const G& g, T* W, int ld, int mw, int n, T* rh
         for (int i = k + 1 + g.rank(); i < mw; i += G::kSize)
             wk[i] *= scale;
         g.sync();
-        // apply H = I - tau v v^T (v_k = 1) to columns k+1..n-1 and to rhs
-        for (int c = k + 1 + g.warp(); c <= n; c += G::kWarps) {
-            T* col = (c < n) ? W + static_cast<size_t>(c) * ld : rhs;
+        // apply H = I - tau v v^T (v_k = 1) to the later columns and the rhs
+        for (int c = k + 1 + g.warp(); c < n + nrhs; c += G::kWarps) {
+            T* col = W + static_cast<size_t>(c) * ld;
             T d = (lane == 0) ? col[k] : T(0);
             for (int i = k + 1 + lane; i < mw; i += 32)
                 d += wk[i] * col[i];
@@ -339,51 +347,104 @@ __device__ void group_normal_correction(const G& g, const T* W, int ld, int n, d
     g.sync();
 }
 
-// FP64 residual r = b - C(I,J) x on I; returns ||r||^2.
+// FP64 residuals r_c = b_c - C(I,J) x_c on I for the nrhs right-hand sides
+// (b_c = B(:, bs * col + c), x_c = x + c * n, r_c = r + c * m); returns the
+// squared Frobenius norm.
 template <class G>
-__device__ double group_residual(const G& g, const Problem& pb, int col, const uint64_t* keys, const int32_t* I, const int32_t* rstart,
-                                 const int32_t* ejj, const double* ev, const double* x, double* r,
-                                 int m)
+__device__ double group_residual(const G& g, const Problem& pb, int col, const uint64_t* keys,
+                                 const int32_t* I, const int32_t* rstart, const int32_t* ejj,
+                                 const double* ev, const double* x, double* r, int m, int n,
+                                 int nrhs)
 {
     double part = 0.0;
-    for (int u = g.rank(); u < m; u += G::kSize) {
-        double v = target_value(pb, col, I[u]);
+    for (int t = g.rank(); t < m * nrhs; t += G::kSize) {
+        const int c = t / m, u = t - c * m;
+        double v = target_value(pb, pb.bs * col + c, I[u]);
+        const double* xc = x + static_cast<size_t>(c) * n;
         for (int i = rstart[u]; i < rstart[u + 1]; i++) {
             const int e = static_cast<int>(keys[i] & kEntryMask);
-            v -= ev[e] * x[ejj[e]];
+            v -= ev[e] * xc[ejj[e]];
         }
-        r[u] = v;
+        r[t] = v;
         part += v * v;
     }
     return g.sum(part);
 }
 
-// Solves column `col`.  `sh` is per-group shared scratch; `s` the slot.
-// Returns nothing; results go to `out`.
+// Solves the 3x3-or-smaller SPD system G Y = N (bs x bs, column-major) by
+// Cholesky in FP64 and returns sum(Y .* N), the block rho term
+// <N, (A_j^T A_j)^-1 N> of Compute_Rhos_Block (src/Spai_Sub.imp:1350-1465).
+__device__ __forceinline__ double block_rho_term(double* Gm, const double* N, int bs)
+{
+    constexpr int kMaxBs = 4;
+    double L[kMaxBs * kMaxBs];
+    for (int j = 0; j < bs; j++) {
+        double d = Gm[j + j * bs];
+        for (int k = 0; k < j; k++)
+            d -= L[j + k * kMaxBs] * L[j + k * kMaxBs];
+        d = sqrt(d);
+        L[j + j * kMaxBs] = d;
+        for (int i = j + 1; i < bs; i++) {
+            double v = Gm[i + j * bs];
+            for (int k = 0; k < j; k++)
+                v -= L[i + k * kMaxBs] * L[j + k * kMaxBs];
+            L[i + j * kMaxBs] = v / d;
+        }
+    }
+    double term = 0.0;
+    for (int q = 0; q < bs; q++) {
+        double y[kMaxBs];
+        for (int i = 0; i < bs; i++) {  // L y = N(:, q)
+            double v = N[i + q * bs];
+            for (int k = 0; k < i; k++)
+                v -= L[i + k * kMaxBs] * y[k];
+            y[i] = v / L[i + i * kMaxBs];
+        }
+        for (int i = bs - 1; i >= 0; i--) {  // L^T z = y
+            double v = y[i];
+            for (int k = i + 1; k < bs; k++)
+                v -= L[k + i * kMaxBs] * y[k];
+            y[i] = v / L[i + i * kMaxBs];
+        }
+        for (int i = 0; i < bs; i++)
+            term += y[i] * N[i + q * bs];
+    }
+    return term;
+}
+
+// Solves problem column `col` (scalar column col, or block column col when
+// pb.bs > 1; then the bs scalar columns bs*col .. bs*col+bs-1 of M share J,
+// I and one QR, with bs right-hand sides).  Results go to `out`.
 template <class T, class G>
 __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slot<T> s,
                              const Output& out, int col)
 {
     const int lane = g.lane();
-    // J <- P(:, col)
+    const int bs = pb.bs;
+    const int nrhs = bs;
+    // J <- P(:, col)   (block indices when bs > 1)
     const int64_t p0 = pb.pptr[col];
-    int n = static_cast<int>(pb.pptr[col + 1] - p0);
+    int nbk = static_cast<int>(pb.pptr[col + 1] - p0);
     int status = 0;
     int steps = 0;
     double res = 0.0;
-    if (n > cap.nmax) {
+    if (nbk * bs > cap.nmax || nrhs > cap.nrhs) {
         status = 3;
-        n = 0;
+        nbk = 0;
     }
-    for (int t = g.rank(); t < n; t += G::kSize)
+    for (int t = g.rank(); t < nbk; t += G::kSize)
         s.J[t] = pb.pidx[p0 + t];
     g.sync();
+    const double ep_eff = pb.ep * sqrt(static_cast<double>(bs));
+    int n = 0;
+    auto scol = [&](int jj) { return bs == 1 ? s.J[jj] : bs * s.J[jj / bs] + jj % bs; };
 
     PHASE_BEGIN();
     for (int step = -1; step < pb.ns && status != 3; step++) {
+        n = nbk * bs;
         // ---- 1. entries of C(:, J), sorted by row
         for (int jj = g.rank(); jj < n; jj += G::kSize) {
-            const int j = s.J[jj];
+            const int j = scol(jj);
             s.off[jj] = static_cast<int>(pb.cptr[j + 1] - pb.cptr[j]);
         }
         g.sync();
@@ -396,7 +457,7 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
         }
         g.sync();
         for (int jj = g.warp(); jj < n; jj += G::kWarps) {
-            const int j = s.J[jj];
+            const int j = scol(jj);
             const int64_t base = pb.cptr[j];
             const int o = s.off[jj];
             const int len = s.off[jj + 1] - o;
@@ -459,15 +520,16 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
             break;
         }
         PHASE_MARK(1);
-        const bool w_smem = s.Wfast && mw * n + mw <= s.wfast_elems;
+        const int wcols = n + nrhs;
+        const bool w_smem = s.Wfast && mw * wcols <= s.wfast_elems;
         T* W = w_smem ? s.Wfast : s.W;
-        T* rhs = W + static_cast<size_t>(mw) * n;  // rhs directly after W
+        T* rhs = W + static_cast<size_t>(mw) * n;  // nrhs columns right after W
         const int ld = mw;
         // blocked QR for CTA groups (panels staged in the shared area when W
         // is in global memory and a panel fits there)
         const bool blocked = (G::kWarps > 1) && s.bsc != nullptr &&
                              (w_smem || (s.Wfast && mw * kPanel <= s.wfast_elems));
-        for (int i = g.rank(); i < mw * n + mw; i += G::kSize)
+        for (int i = g.rank(); i < mw * wcols; i += G::kSize)
             W[i] = T(0);
         g.sync();
         // shared entries
@@ -478,140 +540,225 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
                 const int d = s.tmp[u];
                 W[static_cast<size_t>(s.ejj[e]) * ld + d] = static_cast<T>(s.ev[e]);
                 if (i == s.rstart[u])
-                    rhs[d] = static_cast<T>(target_value(pb, col, s.I[u]));
+                    for (int c = 0; c < nrhs; c++)
+                        rhs[d + static_cast<size_t>(c) * ld] =
+                            static_cast<T>(target_value(pb, bs * col + c, s.I[u]));
             }
         }
         // singleton rows, folded per column (one warp per column)
         for (int jj = g.warp(); jj < n; jj += G::kWarps) {
-            double sig = 0.0, tb = 0.0;
+            double sig = 0.0;
+            double tb[4] = {0.0, 0.0, 0.0, 0.0};
             for (int e = s.off[jj] + lane; e < s.off[jj + 1]; e += 32) {
                 const int u = s.pos[e];
                 if (s.rstart[u + 1] - s.rstart[u] == 1) {
                     const double v = s.ev[e];
                     sig += v * v;
-                    tb += v * target_value(pb, col, s.I[u]);
+#pragma unroll
+                    for (int c = 0; c < 4; c++)
+                        if (c < nrhs)
+                            tb[c] += v * target_value(pb, bs * col + c, s.I[u]);
                 }
             }
             sig = warp_sum(sig);
-            tb = warp_sum(tb);
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+                if (c < nrhs)
+                    tb[c] = warp_sum(tb[c]);
             if (lane == 0) {
                 const double nrm = sqrt(sig);
                 W[static_cast<size_t>(jj) * ld + S + jj] = static_cast<T>(nrm);
-                rhs[S + jj] = static_cast<T>(nrm > 0.0 ? tb / nrm : 0.0);
+                for (int c = 0; c < nrhs; c++)
+                    rhs[S + jj + static_cast<size_t>(c) * ld] =
+                        static_cast<T>(nrm > 0.0 ? tb[c] / nrm : 0.0);
             }
         }
         g.sync();
 
         PHASE_MARK(2);
-        // ---- 3. QR, Q^T b, back substitution
-        int sing;
+        // ---- 3. QR, Q^T b, back substitution (per right-hand side)
+        int sing = 0;
         RView<T> rv{W, ld};
+        T* rhs_s = rhs;
+        int ldr = ld;  // leading dimension of the right-hand sides
         if (blocked) {
-            group_householder_blocked<T>(g, W, ld, mw, n, rhs, w_smem, s.Wfast, s.bsc);
-            if (!w_smem && static_cast<size_t>(n) * (n + 1) / 2 + n <=
+            group_householder_blocked<T>(g, W, ld, mw, n, nrhs, w_smem, s.Wfast, s.bsc);
+            if (!w_smem && static_cast<size_t>(n) * (n + 1) / 2 + static_cast<size_t>(n) * nrhs <=
                                static_cast<size_t>(s.wfast_elems)) {
-                // R (packed) and the right-hand side move to shared memory
+                // R (packed) and the right-hand sides move to shared memory
                 T* rp = s.Wfast;
                 T* rh = s.Wfast + static_cast<size_t>(n) * (n + 1) / 2;
                 group_pack_r<T>(g, W, ld, n, rp);
-                for (int i = g.rank(); i < n; i += G::kSize)
-                    rh[i] = rhs[i];
+                for (int t = g.rank(); t < n * nrhs; t += G::kSize) {
+                    const int c = t / n, i = t - c * n;
+                    rh[t] = rhs[i + static_cast<size_t>(c) * ld];
+                }
                 g.sync();
                 rv = RView<T>{rp, 0};
-                rhs = rh;
+                rhs_s = rh;
+                ldr = n;
             }
             PHASE_MARK(3);
-            sing = group_back_substitute_blocked<T>(g, rv, n, rhs, s.x);
+            for (int c = 0; c < nrhs; c++)
+                sing |= group_back_substitute_blocked<T>(g, rv, n, rhs_s + static_cast<size_t>(c) * ldr,
+                                                         s.x + static_cast<size_t>(c) * n);
         }
         else {
-            group_householder<T>(g, W, ld, mw, n, rhs);
-            sing = group_back_substitute<T>(g, W, ld, n, rhs, s.x);
+            group_householder<T>(g, W, ld, mw, n, nrhs);
+            for (int c = 0; c < nrhs; c++)
+                sing |= group_back_substitute<T>(g, W, ld, n, rhs + static_cast<size_t>(c) * ld,
+                                                 s.x + static_cast<size_t>(c) * n);
         }
         steps++;
-        if (g.rank() == 0) {
-            const double dn = n, dmw = mw, dm = m;
-            double* wk = out.work + 3 * static_cast<size_t>(col);
-            wk[0] += 2.0 * dmw * dn * dn - (2.0 / 3.0) * dn * dn * dn + 4.0 * dmw * dn + 2.0 * E;
-            wk[1] += 2.0 * dm * dn * dn - (2.0 / 3.0) * dn * dn * dn + 4.0 * dm * dn + 2.0 * dm * dn;
-            wk[2] += 12.0 * E + 16.0 * dn + 8.0 * dm;
-        }
         status = sing ? 1 : 0;
+        if (g.rank() == 0) {
+            const double dn = n, dmw = mw, dm = m, dr = nrhs;
+            double* wk = out.work + 3 * static_cast<size_t>(col);
+            wk[0] += 2.0 * dmw * dn * dn - (2.0 / 3.0) * dn * dn * dn + 4.0 * dmw * dn * dr +
+                     2.0 * E * dr;
+            wk[1] += 2.0 * dm * dn * dn - (2.0 / 3.0) * dn * dn * dn + 4.0 * dm * dn * dr +
+                     2.0 * dm * dn * dr;
+            wk[2] += 12.0 * E + 16.0 * dn + 8.0 * dm * dr;
+        }
 
         PHASE_MARK(4);
         // ---- 4/5. refinement (mixed) and FP64 residual
-        double r2 = group_residual(g, pb, col, s.keys, s.I, s.rstart, s.ejj, s.ev, s.x,
-                                   s.r, m);
+        double r2 = group_residual(g, pb, col, s.keys, s.I, s.rstart, s.ejj, s.ev, s.x, s.r, m,
+                                   n, nrhs);
         if (!sing) {
             for (int it = 0; it < pb.refine; it++) {
                 g.sync();
-                for (int jj = g.warp(); jj < n; jj += G::kWarps) {
+                for (int t = g.warp(); t < n * nrhs; t += G::kWarps) {
+                    const int c = t / n, jj = t - c * n;
+                    const double* rc = s.r + static_cast<size_t>(c) * m;
                     double d = 0.0;
                     for (int e = s.off[jj] + lane; e < s.off[jj + 1]; e += 32)
-                        d += s.ev[e] * s.r[s.pos[e]];
+                        d += s.ev[e] * rc[s.pos[e]];
                     d = warp_sum(d);
                     if (lane == 0)
-                        s.gv[jj] = d;
+                        s.gv[t] = d;
                 }
                 g.sync();
-                if (blocked)
-                    group_normal_correction_blocked<T>(g, rv, n, s.gv);
-                else
-                    group_normal_correction<T>(g, W, ld, n, s.gv);
-                for (int jj = g.rank(); jj < n; jj += G::kSize)
-                    s.x[jj] += s.gv[jj];
+                for (int c = 0; c < nrhs; c++) {
+                    if (blocked)
+                        group_normal_correction_blocked<T>(g, rv, n, s.gv + static_cast<size_t>(c) * n);
+                    else
+                        group_normal_correction<T>(g, W, ld, n, s.gv + static_cast<size_t>(c) * n);
+                }
+                for (int t = g.rank(); t < n * nrhs; t += G::kSize)
+                    s.x[t] += s.gv[t];
                 g.sync();
-                r2 = group_residual(g, pb, col, s.keys, s.I, s.rstart, s.ejj, s.ev, s.x,
-                                    s.r, m);
+                r2 = group_residual(g, pb, col, s.keys, s.I, s.rstart, s.ejj, s.ev, s.x, s.r, m,
+                                    n, nrhs);
             }
         }
         res = sqrt(r2);
         g.sync();
         PHASE_MARK(5);
-        if (res <= pb.ep || step == pb.ns - 1)
+        if (res <= ep_eff || step == pb.ns - 1)
             break;
 
-        // ---- 6. pattern update (Augment_Sparsity)
-        // L = I u {col}: candidate entries from the row structure
-        int in_i = 0;
-        {
-            const int u = lower_bound_i32(s.I, m, col);
-            in_i = (u < m && s.I[u] == col) ? 1 : 0;
+        // ---- 6. pattern update (Augment_Sparsity / Augment_Sparsity_Block)
+        // L = I u {col} in rows (bs == 1) or block rows (bs > 1); the
+        // candidate entries are the row structure of L's rows
+        int nl;
+        int32_t* lrows;  // L as (block) row indices
+        if (bs == 1) {
+            int in_i = 0;
+            {
+                const int u = lower_bound_i32(s.I, m, col);
+                in_i = (u < m && s.I[u] == col) ? 1 : 0;
+            }
+            nl = m + (in_i ? 0 : 1);
+            lrows = s.I;
+            if (!in_i && g.rank() == 0)
+                s.pos[0] = col;  // the extra row, read as lrows[m] below
+            g.sync();
         }
-        const int nl = m + (in_i ? 0 : 1);
-        for (int u = g.rank(); u < nl; u += G::kSize) {
-            const int l = (u < m) ? s.I[u] : col;
-            s.tmp[u] = (l < pb.n) ? static_cast<int>(pb.rptr[l + 1] - pb.rptr[l]) : 0;
+        else {
+            // block rows of I (rows < n) are non-decreasing in u
+            for (int u = g.rank(); u < m; u += G::kSize) {
+                const int r = s.I[u];
+                s.tmp[u] = (r < pb.n && (u == 0 || r / bs != s.I[u - 1] / bs)) ? 1 : 0;
+            }
+            g.sync();
+            const int nb_i = group_exclusive_scan(g, s.tmp, m);
+            for (int u = g.rank(); u < m; u += G::kSize) {
+                const int r = s.I[u];
+                if (r < pb.n && (u == 0 || r / bs != s.I[u - 1] / bs))
+                    s.pos[s.tmp[u]] = r / bs;
+            }
+            g.sync();
+            int in_l = 0;
+            {
+                const int q = lower_bound_i32(s.pos, nb_i, col);
+                in_l = (q < nb_i && s.pos[q] == col) ? 1 : 0;
+            }
+            if (!in_l && g.rank() == 0)
+                s.pos[nb_i] = col;
+            nl = nb_i + (in_l ? 0 : 1);
+            lrows = s.pos;
+            g.sync();
+        }
+        // mark the candidate columns in the slot's bit vector; the first thread
+        // to set a bit appends the column to the candidate list (the
+        // reference's bit vector + reset list, src/Spai_Sub.imp:124-200)
+        if (g.rank() == 0)
+            g.sc->i[1] = 0;
+        g.sync();
+        for (int u = g.warp(); u < nl; u += G::kWarps) {
+            int r0, r1;
+            if (bs == 1) {
+                const int l = (u < m) ? lrows[u] : s.pos[0];
+                r0 = l;
+                r1 = (l < pb.n) ? l + 1 : l;
+            }
+            else {
+                const int l = lrows[u];
+                r0 = l * bs;
+                r1 = min(l * bs + bs, pb.n);
+            }
+            for (int r = r0; r < r1; r++) {
+                const int64_t b0 = pb.rptr[r];
+                const int len = static_cast<int>(pb.rptr[r + 1] - b0);
+                for (int t = lane; t < len; t += 32) {
+                    const int c = pb.rcol[b0 + t] / bs;
+                    const uint32_t bit = 1u << (c & 31);
+                    const uint32_t old = atomicOr(&s.bmap[c >> 5], bit);
+                    if (!(old & bit)) {
+                        const int idx = atomicAdd(&g.sc->i[1], 1);
+                        if (idx < cap.cmax)
+                            s.cand[idx] = c;
+                    }
+                }
+            }
         }
         g.sync();
-        const int T_c = group_exclusive_scan(g, s.tmp, nl);
-        if (T_c > cap.cmax) {
+        const int nu = g.sc->i[1];
+        const int T_c = min(nu, cap.cmax);
+        // clear the bit vector for the next use (every set bit is listed)
+        for (int t = g.rank(); t < T_c; t += G::kSize)
+            s.bmap[s.cand[t] >> 5] = 0u;
+        g.sync();
+        if (nu > cap.cmax) {
             status = 3;
             break;
-        }
-        for (int u = g.warp(); u < nl; u += G::kWarps) {
-            const int l = (u < m) ? s.I[u] : col;
-            if (l >= pb.n)
-                continue;
-            const int64_t b0 = pb.rptr[l];
-            const int len = static_cast<int>(pb.rptr[l + 1] - b0);
-            for (int t = lane; t < len; t += 32)
-                s.cand[s.tmp[u] + t] = pb.rcol[b0 + t];
         }
         const int LC = next_pow2(T_c > 0 ? T_c : 1);
         for (int i = T_c + g.rank(); i < LC; i += G::kSize)
             s.cand[i] = 0x7fffffff;
         g.sync();
         group_bitonic_sort(g, s.cand, LC);
-        // keep first occurrences that are not in J (and are in UP(:,col))
+        // keep candidates not in J (and, scalar only, in UP(:,col))
         for (int i = g.rank(); i < T_c; i += G::kSize) {
             const int c = s.cand[i];
-            int keep = (i == 0 || s.cand[i - 1] != c) ? 1 : 0;
-            if (keep) {
-                const int q = lower_bound_i32(s.J, n, c);
-                if (q < n && s.J[q] == c)
+            int keep = 1;
+            {
+                const int q = lower_bound_i32(s.J, nbk, c);
+                if (q < nbk && s.J[q] == c)
                     keep = 0;
             }
-            if (keep && pb.upptr != nullptr) {
+            if (keep && pb.upptr != nullptr && bs == 1) {
                 const int64_t a = pb.upptr[col];
                 const int len = static_cast<int>(pb.upptr[col + 1] - a);
                 const int q = lower_bound_i32(pb.upidx + a, len, c);
@@ -639,26 +786,63 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
         const double res2 = res * res;
         for (int t = g.rank(); t < nt; t += G::kSize) {
             const int j = s.cand[t];
-            double a2 = 0.0, num = 0.0;
-            for (int64_t p = pb.cptr[j]; p < pb.cptr[j + 1]; p++) {
-                const double v = pb.cval[p];
-                a2 += v * v;
-                const int u = lower_bound_i32(s.I, m, pb.cidx[p]);
-                if (u < m && s.I[u] == pb.cidx[p])
-                    num += s.r[u] * v;
+            if (bs == 1) {
+                double a2 = 0.0, num = 0.0;
+                for (int64_t p = pb.cptr[j]; p < pb.cptr[j + 1]; p++) {
+                    const double v = pb.cval[p];
+                    a2 += v * v;
+                    const int u = lower_bound_i32(s.I, m, pb.cidx[p]);
+                    if (u < m && s.I[u] == pb.cidx[p])
+                        num += s.r[u] * v;
+                }
+                const double ajn = sqrt(a2);
+                s.rho[t] = sqrt(res2 - (num * num) / (ajn * ajn));
             }
-            const double ajn = sqrt(a2);
-            s.rho[t] = sqrt(res2 - (num * num) / (ajn * ajn));
+            else {
+                // N = A_j(I)^T R (bs x bs), Gm = A_j^T A_j over the whole block column
+                double N[16], Gm[16];
+                for (int q = 0; q < bs * bs; q++)
+                    N[q] = Gm[q] = 0.0;
+                for (int a = 0; a < bs; a++) {
+                    const int ca = j * bs + a;
+                    for (int64_t p = pb.cptr[ca]; p < pb.cptr[ca + 1]; p++) {
+                        const int u = lower_bound_i32(s.I, m, pb.cidx[p]);
+                        if (u < m && s.I[u] == pb.cidx[p])
+                            for (int b = 0; b < bs; b++)
+                                N[a + b * bs] += pb.cval[p] * s.r[u + static_cast<size_t>(b) * m];
+                    }
+                    for (int a2 = a; a2 < bs; a2++) {
+                        const int cb = j * bs + a2;
+                        int64_t p = pb.cptr[ca], q = pb.cptr[cb];
+                        double gsum = 0.0;
+                        while (p < pb.cptr[ca + 1] && q < pb.cptr[cb + 1]) {
+                            const int rp = pb.cidx[p], rq = pb.cidx[q];
+                            if (rp < rq)
+                                p++;
+                            else if (rp > rq)
+                                q++;
+                            else
+                                gsum += pb.cval[p++] * pb.cval[q++];
+                        }
+                        Gm[a + a2 * bs] = gsum;
+                        Gm[a2 + a * bs] = gsum;
+                    }
+                }
+                const double term = block_rho_term(Gm, N, bs);
+                s.rho[t] = sqrt(res2 - term);
+            }
         }
         {
             // algorithmic work of the candidate scan: 4 flops per entry
             int ce = 0;
             for (int t = g.rank(); t < nt; t += G::kSize)
-                ce += static_cast<int>(pb.cptr[s.cand[t] + 1] - pb.cptr[s.cand[t]]);
+                for (int a = 0; a < bs; a++)
+                    ce += static_cast<int>(pb.cptr[s.cand[t] * bs + a + 1] -
+                                           pb.cptr[s.cand[t] * bs + a]);
             ce = g.sum(ce);
             if (g.rank() == 0) {
-                out.work[3 * static_cast<size_t>(col) + 0] += 4.0 * ce;
-                out.work[3 * static_cast<size_t>(col) + 1] += 4.0 * ce;
+                out.work[3 * static_cast<size_t>(col) + 0] += 4.0 * ce * nrhs;
+                out.work[3 * static_cast<size_t>(col) + 1] += 4.0 * ce * nrhs;
                 out.work[3 * static_cast<size_t>(col) + 2] += 12.0 * ce;
             }
         }
@@ -705,7 +889,7 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
                 if (bt < 0)
                     break;
                 if (lane == 0) {
-                    s.J[n + added] = bj;
+                    s.J[nbk + added] = bj;
                     s.cand[bt] = -1;
                 }
                 added++;
@@ -719,7 +903,7 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
         // keep J sorted (insertion of at most mn new entries, thread 0)
         if (g.rank() == 0) {
             for (int a = 0; a < added; a++) {
-                int q = n + a;
+                int q = nbk + a;
                 const int v = s.J[q];
                 while (q > 0 && s.J[q - 1] > v) {
                     s.J[q] = s.J[q - 1];
@@ -728,44 +912,48 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
                 s.J[q] = v;
             }
         }
-        n += added;
+        nbk += added;
         g.sync();
-        if (n > cap.nmax) {
+        if (nbk * bs > cap.nmax) {
             status = 3;
             break;
         }
     }
+    n = nbk * bs;
 
-    // ---- write column k of M
-    const int64_t o0 = out.optr[col];
-    const int64_t ocap = out.optr[col + 1] - o0;
-    if (status == 3 || n > ocap) {
-        if (g.rank() == 0) {
-            out.olen[col] = 0;
-            out.status[col] = 3;
-            out.res[col] = 0.0;
-            out.steps[col] = steps;
+    // ---- write the bs scalar columns of M for this problem column
+    for (int c = 0; c < bs; c++) {
+        const int sc_col = bs * col + c;
+        const int64_t o0 = out.optr[sc_col];
+        const int64_t ocap = out.optr[sc_col + 1] - o0;
+        if (status == 3 || n > ocap) {
+            if (g.rank() == 0) {
+                out.olen[sc_col] = 0;
+                out.status[sc_col] = 3;
+                out.res[sc_col] = 0.0;
+                out.steps[sc_col] = steps;
+            }
+            continue;
         }
-        g.sync();
-        return;
+        int nonfinite = 0;
+        const double* xc = s.x + static_cast<size_t>(c) * n;
+        for (int t = g.rank(); t < n; t += G::kSize) {
+            const double v = xc[t];
+            if (!isfinite(v))
+                nonfinite = 1;
+            out.oval[o0 + t] = v;
+            if (out.write_idx)
+                out.oidx[o0 + t] = scol(t);
+        }
+        nonfinite = g.sum(nonfinite);
+        if (g.rank() == 0) {
+            out.olen[sc_col] = n;
+            out.res[sc_col] = res;
+            out.steps[sc_col] = steps;
+            out.status[sc_col] = (status == 1) ? 1 : ((nonfinite || !isfinite(res)) ? 2 : 0);
+        }
     }
-    int nonfinite = 0;
-    for (int t = g.rank(); t < n; t += G::kSize) {
-        const double v = s.x[t];
-        if (!isfinite(v))
-            nonfinite = 1;
-        out.oval[o0 + t] = v;
-        if (out.write_idx)
-            out.oidx[o0 + t] = s.J[t];
-    }
-    nonfinite = g.sum(nonfinite);
     PHASE_MARK(6);
-    if (g.rank() == 0) {
-        out.olen[col] = n;
-        out.res[col] = res;
-        out.steps[col] = steps;
-        out.status[col] = (status == 1) ? 1 : ((nonfinite || !isfinite(res)) ? 2 : 0);
-    }
     g.sync();
 }
 

@@ -21,6 +21,10 @@ Cases (reference options in brackets):
                   column, so this pins C = [A; rho Ce] through its default
                   path, whose right-hand side is e_k     [-2 -1 -ns 0 -Ce -Be -rho 10]
   ragged_3000     random nonsymmetric n=3000, P = dropped pattern(A^2) [file -1 -ns 0]
+  block27_6       27-point block stencil 6^3 nodes x 3, block pattern of A
+                                                              [-2 -1 -bs 3 -ns 0]
+  block27_6_upd   same from the diagonal block pattern with block pattern
+                  updates                        [-1 -1 -bs 3 -ns 3 -mn 3 -ep 0.05]
 """
 import os
 import subprocess
@@ -64,6 +68,9 @@ def main():
         ["-2", "-1", "-ns", "0", "-Ce", "Ce.mtx", "-Be", "Be.mtx", "-rho", "10"],
         "aniso16_probe")
     run(W.ragged(3000), ["P.mtx", "-1", "-ns", "0"], "ragged_3000")
+    blk = W.block27(6, probing=False)
+    run(blk, ["-2", "-1", "-bs", "3", "-ns", "0"], "block27_6")
+    run(blk, ["-1", "-1", "-bs", "3", "-ns", "3", "-mn", "3", "-ep", "0.05"], "block27_6_upd")
 
 
 if __name__ == "__main__":

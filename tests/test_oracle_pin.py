@@ -85,3 +85,17 @@ def test_oracle_b_aware_rhs_merges_target():
         I = np.nonzero(np.any(Cd[:, J] != 0, axis=1))[0]
         m, *_ = np.linalg.lstsq(Cd[np.ix_(I, J)], Bd[I, k], rcond=None)
         assert np.allclose(r.M[:, k].toarray().ravel()[J], m, rtol=1e-12, atol=1e-14)
+
+
+@pytest.mark.parametrize("name,kind,kw", [
+    ("block27_6", "A", dict(ns=0)),
+    ("block27_6_upd", "diag", dict(ns=3, mn=3, ep=0.05)),
+])
+def test_block_spai(name, kind, kw):
+    """Block SPAI (-bs 3) against the reference's block path."""
+    w = W.block27(6, probing=False)
+    Pb = O.block_pattern(w.A, 3) if kind == "A" else sp.identity(w.n // 3, format="csc")
+    r = O.spai_block(w.A, Pb, 3, **kw)
+    ref = load_golden(name)
+    assert same_pattern(r.M, ref)
+    assert max_rel_diff(r.M, ref) < PRINT_TOL
