@@ -30,6 +30,9 @@ struct BlockedScratch {
     T tmat[kPanel * kPanel];  // T factor (upper triangular, column-major)
     T tau[kPanel];
     T vtv[kPanel * kPanel];   // V^T V (strictly upper part used)
+    T scale[kPanel];          // 1 / (alpha - beta) of each panel column
+    T beta[kPanel];           // R(k, k) of each panel column
+    T nrm2[kPanel + 1];       // squared norm below the diagonal, next column
 };
 
 // V(r, i) of the panel: unit lower trapezoidal, explicit below the diagonal.
@@ -280,6 +283,165 @@ __device__ void trailing_update(const G& g, const T* P, int ldp, int mp, int nb,
     }
 }
 
+// Unblocked Householder QR of the panel P (mp x nb, ld ldp) with one group
+// barrier per column: the norm of column k+1 below its diagonal is computed by
+// the warp that updates column k+1 during step k, the dot products of step k
+// use the unscaled column k (v = scale * x), and the scaling of every panel
+// column and its diagonal entry beta are applied once after the last step.
+// Same reflectors as panel_qr (LAPACK dlarfg convention).
+template <class T, class G>
+__device__ void panel_qr_fast(const G& g, T* P, int ldp, int mp, int nb, BlockedScratch<T>* bs)
+{
+    const int lane = g.lane();
+    {
+        T part = 0;
+        for (int i = 1 + g.rank(); i < mp; i += G::kSize)
+            part += P[i] * P[i];
+        const T x2 = g.sum(part);
+        if (g.rank() == 0)
+            bs->nrm2[0] = x2;
+    }
+    g.sync();
+    for (int k = 0; k < nb; k++) {
+        const T* pk = P + static_cast<size_t>(k) * ldp;
+        const T alpha = pk[k];
+        const T x2 = bs->nrm2[k];
+        T tau = 0, scale = 0, beta = alpha;
+        if (x2 != T(0)) {
+            beta = -copysign(tsqrt<T>(alpha * alpha + x2), alpha);
+            tau = (beta - alpha) / beta;
+            scale = T(1) / (alpha - beta);
+        }
+        for (int c = k + 1 + g.warp(); c < nb; c += G::kWarps) {
+            T* col = P + static_cast<size_t>(c) * ldp;
+            if (tau != T(0)) {
+                T d = 0;
+                for (int i = k + 1 + lane; i < mp; i += 32)
+                    d += pk[i] * col[i];
+                d = (col[k] + scale * warp_sum(d)) * tau;
+                if (lane == 0)
+                    col[k] -= d;
+                const T ds = d * scale;
+                for (int i = k + 1 + lane; i < mp; i += 32)
+                    col[i] -= ds * pk[i];
+            }
+            if (c == k + 1) {
+                T q = 0;
+                for (int i = k + 2 + lane; i < mp; i += 32)
+                    q += col[i] * col[i];
+                q = warp_sum(q);
+                if (lane == 0)
+                    bs->nrm2[k + 1] = q;
+            }
+        }
+        if (g.rank() == 0) {
+            bs->tau[k] = tau;
+            bs->scale[k] = scale;
+            bs->beta[k] = beta;
+        }
+        g.sync();
+    }
+    // deferred: v = scale * x below the diagonal, R(k, k) = beta
+    for (int t = g.rank(); t < nb * mp; t += G::kSize) {
+        const int k = t / mp, i = t - k * mp;
+        T* pk = P + static_cast<size_t>(k) * ldp;
+        if (i > k && bs->tau[k] != T(0))
+            pk[i] *= bs->scale[k];
+        else if (i == k)
+            pk[i] = bs->beta[k];
+    }
+    g.sync();
+}
+
+// Applies the panel's reflectors H_0 .. H_{nb-1} (V unit lower trapezoidal in
+// P, tau in bs) to `ncols` columns of W2 (ld ldw; right-hand sides included).
+// One warp owns NC columns and holds them in registers (Q rows per lane, rows
+// lane + 32 q) for all nb reflectors: each column is read and written once
+// per panel, and every V element loaded from shared memory serves NC columns.
+template <class T, class G, int Q, int NC>
+__device__ void trailing_apply_q(const G& g, const T* P, int ldp, int mp, int nb,
+                                 const BlockedScratch<T>* bs, T* W2, int ldw, int ncols)
+{
+    const int lane = g.lane();
+    for (int cb = g.warp() * NC; cb < ncols; cb += G::kWarps * NC) {
+        T* cp[NC];
+#pragma unroll
+        for (int c = 0; c < NC; c++)
+            cp[c] = (cb + c < ncols) ? W2 + static_cast<size_t>(cb + c) * ldw : nullptr;
+        T x[NC][Q];
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+            const int r = lane + 32 * q;
+#pragma unroll
+            for (int c = 0; c < NC; c++)
+                x[c][q] = (cp[c] && r < mp) ? cp[c][r] : T(0);
+        }
+        for (int k = 0; k < nb; k++) {
+            const T tau = bs->tau[k];
+            if (tau == T(0))
+                continue;
+            const T* pk = P + static_cast<size_t>(k) * ldp;
+            T vq[Q];
+            // row lane of the first 32 holds the unit diagonal / zeros above
+            vq[0] = (lane > k && lane < mp) ? pk[lane] : (lane == k ? T(1) : T(0));
+#pragma unroll
+            for (int q = 1; q < Q; q++) {
+                const int r = lane + 32 * q;
+                vq[q] = (r < mp) ? pk[r] : T(0);
+            }
+            T d[NC];
+#pragma unroll
+            for (int c = 0; c < NC; c++) {
+                T a = 0;
+#pragma unroll
+                for (int q = 0; q < Q; q++)
+                    a += vq[q] * x[c][q];
+                d[c] = a;
+            }
+#pragma unroll
+            for (int c = 0; c < NC; c++)
+                d[c] = warp_sum(d[c]) * tau;
+#pragma unroll
+            for (int c = 0; c < NC; c++)
+#pragma unroll
+                for (int q = 0; q < Q; q++)
+                    x[c][q] -= d[c] * vq[q];
+        }
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+            const int r = lane + 32 * q;
+            if (r < mp) {
+#pragma unroll
+                for (int c = 0; c < NC; c++)
+                    if (cp[c])
+                        cp[c][r] = x[c][q];
+            }
+        }
+    }
+}
+
+// Dispatch on the rows per lane: the smallest Q (in steps of 4) with
+// 32 Q >= mp; four columns per warp tile for short panels, two otherwise.
+template <class T, class G>
+__device__ bool trailing_apply(const G& g, const T* P, int ldp, int mp, int nb,
+                               const BlockedScratch<T>* bs, T* W2, int ldw, int ncols)
+{
+    const int q = (mp + 31) / 32;
+    if (q <= 4)
+        trailing_apply_q<T, G, 4, 4>(g, P, ldp, mp, nb, bs, W2, ldw, ncols);
+    else if (q <= 8)
+        trailing_apply_q<T, G, 8, 4>(g, P, ldp, mp, nb, bs, W2, ldw, ncols);
+    else if (q <= 12)
+        trailing_apply_q<T, G, 12, 2>(g, P, ldp, mp, nb, bs, W2, ldw, ncols);
+    else if (q <= 16)
+        trailing_apply_q<T, G, 16, 2>(g, P, ldp, mp, nb, bs, W2, ldw, ncols);
+    else if (q <= 24)
+        trailing_apply_q<T, G, 24, 1>(g, P, ldp, mp, nb, bs, W2, ldw, ncols);
+    else
+        return false;
+    return true;
+}
+
 // Blocked Householder QR of W (mw x n, ld) applied to the nrhs right-hand
 // sides stored as the next columns of W.  `region` is a shared-memory area of
 // at least mw * kPanel elements used to stage panels when W is not itself in
@@ -308,8 +470,10 @@ __device__ void group_householder_blocked(const G& g, T* W, int ld, int mw, int 
             }
             g.sync();
         }
-        panel_qr<T>(g, P, ldp, mp, nb, bs->tau);
-        panel_tfactor<T>(g, P, ldp, mp, nb, bs);
+        panel_qr_fast<T>(g, P, ldp, mp, nb, bs);
+        const bool reg_path = mp <= 32 * 24;
+        if (!reg_path)
+            panel_tfactor<T>(g, P, ldp, mp, nb, bs);  // compact WY for tall panels
         if (!w_in_smem) {
             // only R (rows < nb of the panel) is needed later
             for (int t = g.rank(); t < nb * nb; t += G::kSize) {
@@ -318,8 +482,10 @@ __device__ void group_householder_blocked(const G& g, T* W, int ld, int mw, int 
                     Wc[r + static_cast<size_t>(c) * ld] = P[r + c * mp];
             }
         }
-        trailing_update<T>(g, P, ldp, mp, nb, bs, W + static_cast<size_t>(c0 + nb) * ld + c0, ld,
-                           n - c0 - nb + nrhs);
+        T* W2 = W + static_cast<size_t>(c0 + nb) * ld + c0;
+        const int ncols = n - c0 - nb + nrhs;
+        if (!reg_path || !trailing_apply<T>(g, P, ldp, mp, nb, bs, W2, ld, ncols))
+            trailing_update<T>(g, P, ldp, mp, nb, bs, W2, ld, ncols);
         g.sync();
     }
 }
