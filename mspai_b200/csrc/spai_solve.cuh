@@ -645,11 +645,21 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
                     else
                         group_normal_correction<T>(g, W, ld, n, s.gv + static_cast<size_t>(c) * n);
                 }
-                for (int t = g.rank(); t < n * nrhs; t += G::kSize)
-                    s.x[t] += s.gv[t];
-                g.sync();
+                double d2 = 0.0, x2 = 0.0;
+                for (int t = g.rank(); t < n * nrhs; t += G::kSize) {
+                    const double x1 = s.x[t] + s.gv[t];
+                    d2 += s.gv[t] * s.gv[t];
+                    x2 += x1 * x1;
+                    s.x[t] = x1;
+                }
+                d2 = g.sum(d2);
+                x2 = g.sum(x2);
                 r2 = group_residual(g, pb, col, s.keys, s.I, s.rstart, s.ejj, s.ev, s.x, s.r, m,
                                     n, nrhs);
+                // converged: ||delta|| <= 2^-44 ||x||; the next correction would be
+                // smaller again by about kappa^2 * u_fp32, far below FP64 rounding
+                if (d2 <= 0x1p-88 * x2)
+                    break;
             }
         }
         res = sqrt(r2);
