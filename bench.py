@@ -297,8 +297,10 @@ def bench_ours(args):
     prof = os.path.join(HERE, "profiles", "ragged_solve_traffic.json")
     if os.path.exists(prof):
         try:
+            # DRAM bytes of one captured launch, scaled to this launch by the
+            # columns it solves (traffic grows with the columns processed)
             pj = json.load(open(prof))
-            traffic = pj.get("dram_bytes_per_launch_scaled")
+            traffic = pj["dram_bytes_per_column"] * st["bucket_columns"][b]
         except Exception:
             traffic = None
     roofline = {"bound": "fp32", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
