@@ -84,9 +84,9 @@ typedef struct {
     int32_t ns;       /* -ns  max update steps (5); 0 = fixed pattern         */
     int32_t um;       /* -um  1: candidates need rho <= mean, 0: <= sum (1)   */
     int32_t hs;       /* -hs  remote-column hash size 0..6 (accepted, unused) */
-    int32_t cs;       /* -cs  cache size (0); > 0 enables the QR reuse table  */
+    int32_t cs;       /* -cs  cache size (0); > 0: reuse table of <= cs problems */
     int32_t qr;       /* -qr  0..5 QR-update mode (accepted; dense on GPU)    */
-    int32_t ch;       /* -ch  0/1 hashing (maps to the QR reuse table)        */
+    int32_t ch;       /* -ch  0/1 reuse table without a size limit            */
     double fg;        /* -fg  fill grade for -qr 1 (accepted)                  */
     int32_t pk;       /* -pk  prefetch count (accepted, unused on one GPU)    */
     int32_t pm;       /* -pm  prefetch all (accepted, unused on one GPU)      */
@@ -121,6 +121,7 @@ typedef struct {
     double kernel_ms[4];      /* device time per bucket kernel               */
     int64_t kernel_launches;  /* kernels this library launched in the setup  */
     double bucket_flops[4];   /* algorithmic (folded) flops per bucket kernel */
+    int64_t reused_columns;   /* columns that took an identical column's solution (-cs/-ch) */
 } mspai_stats;
 
 typedef struct mspai_handle mspai_handle;

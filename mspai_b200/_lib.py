@@ -45,7 +45,8 @@ class mspai_stats(ctypes.Structure):
                 ("flops", ctypes.c_double), ("flops_dense", ctypes.c_double),
                 ("gather_bytes", ctypes.c_double), ("setup_ms", ctypes.c_double),
                 ("kernel_ms", ctypes.c_double * 4), ("kernel_launches", ctypes.c_int64),
-                ("bucket_flops", ctypes.c_double * 4)]
+                ("bucket_flops", ctypes.c_double * 4),
+                ("reused_columns", ctypes.c_int64)]
 
 
 class mspai_matrix(ctypes.Structure):

@@ -223,6 +223,7 @@ class Handle:
             "flops_dense": s.flops_dense, "gather_bytes": s.gather_bytes,
             "setup_ms": s.setup_ms, "kernel_ms": list(s.kernel_ms)[:3],
             "kernel_launches": s.kernel_launches, "bucket_flops": list(s.bucket_flops)[:3],
+            "reused_columns": s.reused_columns,
         }
 
     def adjoint(self, C: MatrixLike, B: Optional[MatrixLike] = None,

@@ -79,6 +79,7 @@ struct mspai_handle {
     DevBuf oidx, oval, olen, res, steps, status, work;
     DevBuf mptr, midx, mval;  // final M
     DevBuf scratch;
+    DevBuf rkeys, rslot_rep, rslot_of, rrep;  // reuse table
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t evb[2 * kBuckets] = {};
     // result description
@@ -437,8 +438,30 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     h->launches++;
     CUDA_TRY(h, mspai::launch_plan(pb.cptr, pb.pptr, pb.pidx, nprob, bs, h->E.as<int32_t>(),
                                    h->nk.as<int32_t>(), st));
+    // ---- reuse of identical problems (-cs / -ch): fixed scalar patterns
+    const bool reuse = (prm->cs > 0 || prm->ch > 0) && !adaptive && bs == 1 && prm->batched;
+    int32_t* drep = nullptr;
+    if (reuse) {
+        const int max_keys = prm->cs > 0 ? prm->cs : nprob;
+        const size_t slots = mspai::reuse_table_slots(nprob, max_keys);
+        CUDA_TRY(h, h->rkeys.ensure(sizeof(uint64_t) * slots));
+        CUDA_TRY(h, h->rslot_rep.ensure(sizeof(int32_t) * slots));
+        CUDA_TRY(h, h->rslot_of.ensure(sizeof(int32_t) * std::max(nprob, 1)));
+        CUDA_TRY(h, h->rrep.ensure(sizeof(int32_t) * std::max(nprob, 1)));
+        mspai::ReuseTable tab{};
+        tab.keys = h->rkeys.as<uint64_t>();
+        tab.rep_of_slot = h->rslot_rep.as<int32_t>();
+        tab.slot_of = h->rslot_of.as<int32_t>();
+        tab.nkeys = dcnt + 20;
+        tab.mask = static_cast<uint32_t>(slots - 1);
+        tab.max_keys = max_keys;
+        drep = h->rrep.as<int32_t>();
+        h->launches += 2;
+        CUDA_TRY(h, mspai::launch_reuse_keys(pb, nprob, tab, drep, dcnt + 21, st));
+    }
     CUDA_TRY(h, cudaStreamSynchronize(st));  // max_col_nnz is on the host now
     BucketRule rule{};
+    rule.rep = drep;
     rule.single_bucket = prm->batched ? -1 : 2;
     rule.allow_warp = (adaptive || bs > 1) ? 0 : 1;
     rule.warp_emax = 64;
@@ -515,6 +538,11 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
         CUDA_TRY(h, cudaEventRecord(h->evb[2 * b + 1], st));
     }
 
+    if (reuse) {
+        h->launches++;
+        CUDA_TRY(h, mspai::launch_reuse_copy(drep, nprob, out, st));
+    }
+
     // ---- assemble M
     if (compact) {
         CUDA_TRY(h, h->mptr.ensure(sizeof(int64_t) * (n + 1)));
@@ -568,6 +596,12 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
             cudaEventElapsedTime(&kms, h->evb[2 * b], h->evb[2 * b + 1]);
             h->stats.kernel_ms[b] = kms;
         }
+    }
+    h->stats.reused_columns = 0;
+    if (reuse) {
+        int32_t nre = 0;
+        CUDA_TRY(h, cudaMemcpy(&nre, dcnt + 21, sizeof(int32_t), cudaMemcpyDeviceToHost));
+        h->stats.reused_columns = nre;
     }
     h->stats.columns = n;
     h->nprob = nprob;

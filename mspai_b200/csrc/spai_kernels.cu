@@ -67,6 +67,8 @@ __global__ void bucket_kernel(const int32_t* __restrict__ E, const int32_t* __re
 {
     for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < n;
          col += gridDim.x * blockDim.x) {
+        if (rule.rep && rule.rep[col] != col)
+            continue;  // solved by its representative
         // sizes after at most ns pattern updates
         const int64_t nf = static_cast<int64_t>(nk[col]) + rule.grow_n;
         const int64_t ef = static_cast<int64_t>(E[col]) + rule.grow_e;
@@ -231,6 +233,8 @@ __global__ void max_len_kernel(const int64_t* __restrict__ ptr, int n, int32_t* 
 // ------------------------------------------------------------------ launchers
 namespace {
 int g_num_sms = 0;
+}  // namespace
+
 int num_sms()
 {
     if (g_num_sms == 0) {
@@ -242,7 +246,6 @@ int num_sms()
     }
     return g_num_sms;
 }
-}  // namespace
 
 cudaError_t launch_plan(const int64_t* cptr, const int64_t* pptr, const int32_t* pidx, int nprob,
                         int bs, int32_t* E, int32_t* nk, cudaStream_t st)

@@ -23,6 +23,7 @@ struct BucketRule {
     int elem_bytes;        // 4 (mixed) or 8 (FP64)
     int grow_n;            // mn * ns
     int grow_e;            // mn * ns * max column nnz of C
+    const int32_t* rep;    // reuse table: columns with rep[k] != k are skipped (nullable)
 };
 
 // E[k] = entries of C in the (scalar) columns of problem column k, nk[k] =
@@ -54,6 +55,24 @@ cudaError_t launch_compact(const int64_t* cap_ptr, const int32_t* cidx, const do
                            const int64_t* out_ptr, int32_t* oidx, double* oval, int n,
                            cudaStream_t st);
 cudaError_t launch_max_len(const int64_t* ptr, int n, int32_t* out, cudaStream_t st);
+
+int num_sms();
+
+// Reuse of identical least-squares problems (reuse.cu).
+struct ReuseTable {
+    uint64_t* keys;         // mask + 1 slots, 0 = empty
+    int32_t* rep_of_slot;   // smallest column with the slot's key
+    int32_t* slot_of;       // per column: its slot or -1
+    int32_t* nkeys;         // distinct keys stored
+    uint32_t mask;          // slots - 1 (power of two)
+    int32_t max_keys;       // cache size: at most this many distinct problems
+};
+size_t reuse_table_slots(int nprob, int max_keys);
+// rep[k] = the column whose solution column k takes (k: solved itself);
+// *nreused = columns with rep[k] != k
+cudaError_t launch_reuse_keys(const Problem& pb, int nprob, const ReuseTable& t, int32_t* rep,
+                              int32_t* nreused, cudaStream_t st);
+cudaError_t launch_reuse_copy(const int32_t* rep, int nprob, const Output& out, cudaStream_t st);
 
 // Adjoint of the fixed-pattern setup (adjoint.cu).
 struct AdjointIO {
