@@ -146,9 +146,14 @@ __global__ void reuse_key_kernel(Problem pb, int nprob, ReuseTable t)
             int slot = -1;
             uint32_t s = static_cast<uint32_t>(h ^ (h >> 32)) & t.mask;
             // at most max_keys distinct problems are stored (the cache size);
-            // a column that finds no place is solved on its own
+            // a column that finds no place is solved on its own.  Best effort:
+            // a column that sees its key's slot still empty while the table
+            // is full (the key being inserted at that moment) also solves on
+            // its own, which changes no result.
             for (uint32_t probe = 0; probe <= t.mask; probe++) {
-                const unsigned long long cur = t.keys[s];
+                // read through L2: other warps insert concurrently
+                const unsigned long long cur = __ldcg(
+                    reinterpret_cast<const unsigned long long*>(t.keys) + s);
                 if (cur == h) {
                     slot = static_cast<int>(s);
                     break;
