@@ -620,4 +620,95 @@ __device__ void group_normal_correction_blocked(const G& g, RView<T> R, int n, d
     }
 }
 
+// rinv[j] = 1 / R(j, j) in FP64 (R nonsingular), for the corrections below.
+template <class T, class G>
+__device__ void group_diag_reciprocals(const G& g, RView<T> R, int n, double* rinv)
+{
+    for (int j = g.rank(); j < n; j += G::kSize)
+        rinv[j] = 1.0 / static_cast<double>(R(j, j));
+    g.sync();
+}
+
+// gv <- R^-1 R^-T gv in FP64 (R in T, rinv = 1 / diag(R)), right-looking by
+// 16-column blocks: one warp solves a block's diagonal triangle with the
+// block's values in lanes (a shuffle and an FMA per step, the block's column
+// of R prefetched into registers), then every thread updates one remaining
+// entry with the block's 16 solved values.  Two barriers per block.
+template <class T, class G>
+__device__ void group_normal_correction_rl(const G& g, RView<T> R, int n, const double* rinv,
+                                           double* gv)
+{
+    const int lane = g.lane();
+    // forward R^T z = g: z_j = (g_j - sum_{i<j} R(i,j) z_i) / R(j,j)
+    for (int c0 = 0; c0 < n; c0 += kPanel) {
+        const int nb = min(kPanel, n - c0);
+        if (g.warp() == 0) {
+            const int i = c0 + lane;  // this lane's entry (lanes < nb)
+            double gi = lane < nb ? gv[i] : 0.0;
+            double rc[kPanel];        // R(c0 + j, i) for j < lane
+#pragma unroll
+            for (int j = 0; j < kPanel; j++)
+                rc[j] = (j < lane && lane < nb) ? static_cast<double>(R(c0 + j, i)) : 0.0;
+            const double ri = lane < nb ? rinv[i] : 0.0;
+#pragma unroll
+            for (int j = 0; j < kPanel; j++) {
+                if (j >= nb)
+                    break;
+                if (lane == j)
+                    gi *= ri;
+                const double zj = __shfl_sync(0xffffffffu, gi, j);
+                if (lane > j)
+                    gi -= rc[j] * zj;
+            }
+            if (lane < nb)
+                gv[i] = gi;
+        }
+        g.sync();
+        const int c1 = c0 + nb;
+        for (int j = c1 + g.rank(); j < n; j += G::kSize) {
+            double acc = 0.0;
+#pragma unroll 4
+            for (int i = c0; i < c1; i++)
+                acc += static_cast<double>(R(i, j)) * gv[i];
+            gv[j] -= acc;
+        }
+        g.sync();
+    }
+    // backward R d = z: d_j = (z_j - sum_{i>j} R(j,i) d_i) / R(j,j)
+    for (int c1 = n; c1 > 0; c1 -= kPanel) {
+        const int c0 = max(0, c1 - kPanel);
+        const int nb = c1 - c0;
+        if (g.warp() == 0) {
+            const int i = c0 + lane;
+            double zi = lane < nb ? gv[i] : 0.0;
+            double rr[kPanel];        // R(i, c0 + j) for j > lane
+#pragma unroll
+            for (int j = 0; j < kPanel; j++)
+                rr[j] = (j > lane && j < nb) ? static_cast<double>(R(i, c0 + j)) : 0.0;
+            const double ri = lane < nb ? rinv[i] : 0.0;
+#pragma unroll
+            for (int j = kPanel - 1; j >= 0; j--) {
+                if (j >= nb)
+                    continue;
+                if (lane == j)
+                    zi *= ri;
+                const double dj = __shfl_sync(0xffffffffu, zi, j);
+                if (lane < j)
+                    zi -= rr[j] * dj;
+            }
+            if (lane < nb)
+                gv[i] = zi;
+        }
+        g.sync();
+        for (int i = g.rank(); i < c0; i += G::kSize) {
+            double acc = 0.0;
+#pragma unroll 4
+            for (int j = c0; j < c1; j++)
+                acc += static_cast<double>(R(i, j)) * gv[j];
+            gv[i] -= acc;
+        }
+        g.sync();
+    }
+}
+
 }  // namespace mspai

@@ -121,6 +121,9 @@ struct Slot {
     BlockedScratch<T>* bsc;  // shared scratch of the blocked QR (CTA groups)
     double* x;         // nmax  solution
     double* gv;        // nmax  refinement right-hand side / correction
+    double* rinv;      // nmax  1 / R(j, j) in FP64
+    double* rs;        // (emax / 2 + 1) * nrhs  residual on the shared rows
+    int32_t* srow;     // emax / 2 + 1  position in I of each shared row
     int32_t* cand;     // lcand candidate column indices (adaptive)
     int32_t* ctmp;     // cmax + 1 candidate flags / scan
     uint32_t* bmap;    // nbmap words: bit vector over problem columns (adaptive)
@@ -137,7 +140,7 @@ __host__ __device__ inline size_t align_up(size_t v, size_t a)
 template <class T>
 struct SlotLayout {
     size_t o_J, o_off, o_ejj, o_ev, o_pos, o_keys, o_I, o_rstart, o_tmp, o_r, o_W, o_rhs, o_x,
-        o_gv, o_cand, o_ctmp, o_rho, o_bmap, bytes;
+        o_gv, o_rinv, o_rs, o_srow, o_cand, o_ctmp, o_rho, o_bmap, bytes;
     __host__ __device__ SlotLayout(const Caps& c, bool w_external)
     {
         size_t o = 0;
@@ -153,6 +156,9 @@ struct SlotLayout {
         o_r = take(sizeof(double) * static_cast<size_t>(c.emax) * nr);
         o_x = take(sizeof(double) * static_cast<size_t>(c.nmax) * nr);
         o_gv = take(sizeof(double) * static_cast<size_t>(c.nmax) * nr);
+        o_rinv = take(sizeof(double) * c.nmax);
+        o_rs = take(sizeof(double) * static_cast<size_t>(c.emax / 2 + 1) * nr);
+        o_srow = take(sizeof(int32_t) * (c.emax / 2 + 1));
         o_rho = take(sizeof(double) * (c.cmax > 0 ? c.cmax : 1));
         o_J = take(sizeof(int32_t) * c.nmax);
         o_off = take(sizeof(int32_t) * (c.nmax + 1));
@@ -188,6 +194,9 @@ struct SlotLayout {
         s.r = reinterpret_cast<double*>(base + o_r);
         s.x = reinterpret_cast<double*>(base + o_x);
         s.gv = reinterpret_cast<double*>(base + o_gv);
+        s.rinv = reinterpret_cast<double*>(base + o_rinv);
+        s.rs = reinterpret_cast<double*>(base + o_rs);
+        s.srow = reinterpret_cast<int32_t*>(base + o_srow);
         s.cand = reinterpret_cast<int32_t*>(base + o_cand);
         s.ctmp = reinterpret_cast<int32_t*>(base + o_ctmp);
         s.bmap = reinterpret_cast<uint32_t*>(base + o_bmap);
@@ -367,6 +376,63 @@ __device__ double group_residual(const G& g, const Problem& pb, int col, const u
         }
         r[t] = v;
         part += v * v;
+    }
+    return g.sum(part);
+}
+
+// Fixed-pattern refinement residual: r = b - C(I,J) x in FP64 and the
+// gradient gv = C(I,J)^T r, for the nrhs right-hand sides, in one pass over
+// the entries (no pass over the rows of I).  `code[e]` is -1 for an entry that
+// is alone in its row (its residual b_e - v_e x_j is formed in place, b_e in
+// `eb[c * estride + e]`) and the dense shared-row number d otherwise; the S
+// shared rows (positions srow[d] in I) are done first, one thread per row.
+// A thread per column sums its entries in order, so the result does not
+// depend on the schedule.  Returns ||r||_F^2.
+template <class G>
+__device__ double group_residual_gradient(const G& g, const Problem& pb, int col,
+                                          const uint64_t* keys, const int32_t* I,
+                                          const int32_t* rstart, const int32_t* srow,
+                                          const int32_t* off, const int32_t* ejj,
+                                          const double* ev, const int32_t* code,
+                                          const double* eb, int estride, const double* x,
+                                          double* rs, double* gv, int S, int n, int nrhs)
+{
+    double part = 0.0;
+    for (int t = g.rank(); t < S * nrhs; t += G::kSize) {
+        const int c = t / S, d = t - c * S;
+        const int u = srow[d];
+        double v = target_value(pb, pb.bs * col + c, I[u]);
+        const double* xc = x + static_cast<size_t>(c) * n;
+        for (int i = rstart[u]; i < rstart[u + 1]; i++) {
+            const int e = static_cast<int>(keys[i] & kEntryMask);
+            v -= ev[e] * xc[ejj[e]];
+        }
+        rs[t] = v;
+        part += v * v;
+    }
+    g.sync();
+    for (int t = g.rank(); t < n * nrhs; t += G::kSize) {
+        const int c = t / n, jj = t - c * n;
+        const double xj = x[t];
+        const double* ebc = eb + static_cast<size_t>(c) * estride;
+        const double* rsc = rs + static_cast<size_t>(c) * S;
+        double acc = 0.0;
+        const int e1 = off[jj + 1];
+#pragma unroll 4
+        for (int e = off[jj]; e < e1; e++) {
+            const double v = ev[e];
+            const int cd = code[e];
+            double r;
+            if (cd < 0) {
+                r = ebc[e] - v * xj;
+                part += r * r;
+            }
+            else {
+                r = rsc[cd];
+            }
+            acc += v * r;
+        }
+        gv[t] = acc;
     }
     return g.sum(part);
 }
@@ -574,6 +640,25 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
             }
         }
         g.sync();
+        // fixed pattern: per-entry codes for the refinement pass; `pos` is not
+        // needed afterwards and takes the codes (-1 or the shared row), the
+        // residual area holds the right-hand side of every singleton entry
+        const bool fixed = (pb.ns == 0);
+        if (fixed) {
+            for (int e = g.rank(); e < E; e += G::kSize) {
+                const int u = s.pos[e];
+                const bool shared = (s.rstart[u + 1] - s.rstart[u]) >= 2;
+                if (!shared)
+                    for (int c = 0; c < nrhs; c++)
+                        s.r[static_cast<size_t>(c) * cap.emax + e] =
+                            target_value(pb, bs * col + c, s.I[u]);
+                s.pos[e] = shared ? s.tmp[u] : -1;
+            }
+            for (int u = g.rank(); u < m; u += G::kSize)
+                if (s.rstart[u + 1] - s.rstart[u] >= 2)
+                    s.srow[s.tmp[u]] = u;
+            g.sync();
+        }
 
         PHASE_MARK(2);
         // ---- 3. QR, Q^T b, back substitution (per right-hand side)
@@ -623,9 +708,41 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
 
         PHASE_MARK(4);
         // ---- 4/5. refinement (mixed) and FP64 residual
-        double r2 = group_residual(g, pb, col, s.keys, s.I, s.rstart, s.ejj, s.ev, s.x, s.r, m,
-                                   n, nrhs);
-        if (!sing) {
+        double r2 = 0.0;
+        if (fixed) {
+            // one pass over the entries gives ||r||^2 and C^T r
+            const RView<T> rq = blocked ? rv : RView<T>{W, ld};
+            auto resid_grad = [&]() {
+                return group_residual_gradient(g, pb, col, s.keys, s.I, s.rstart, s.srow, s.off,
+                                               s.ejj, s.ev, s.pos, s.r, cap.emax, s.x, s.rs,
+                                               s.gv, S, n, nrhs);
+            };
+            r2 = resid_grad();
+            if (!sing && pb.refine > 0) {
+                group_diag_reciprocals<T>(g, rq, n, s.rinv);
+                for (int it = 0; it < pb.refine; it++) {
+                    for (int c = 0; c < nrhs; c++)
+                        group_normal_correction_rl<T>(g, rq, n, s.rinv,
+                                                      s.gv + static_cast<size_t>(c) * n);
+                    double d2 = 0.0, x2 = 0.0;
+                    for (int t = g.rank(); t < n * nrhs; t += G::kSize) {
+                        const double x1 = s.x[t] + s.gv[t];
+                        d2 += s.gv[t] * s.gv[t];
+                        x2 += x1 * x1;
+                        s.x[t] = x1;
+                    }
+                    d2 = g.sum(d2);
+                    x2 = g.sum(x2);
+                    r2 = resid_grad();
+                    if (d2 <= 0x1p-88 * x2)
+                        break;
+                }
+            }
+        }
+        else
+            r2 = group_residual(g, pb, col, s.keys, s.I, s.rstart, s.ejj, s.ev, s.x, s.r, m, n,
+                                nrhs);
+        if (!sing && !fixed) {
             for (int it = 0; it < pb.refine; it++) {
                 g.sync();
                 for (int t = g.warp(); t < n * nrhs; t += G::kWarps) {
