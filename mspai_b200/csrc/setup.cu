@@ -525,7 +525,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
             size_t wsm = std::min<size_t>(mspai::w_bytes(cap, elem), h->smem_budget);
             if (!prm->batched)
                 wsm = 0;  // the plain path keeps W in global memory, unblocked
-            const size_t need = mspai::cta_scratch_needed(elem, cap, count);
+            const size_t need = mspai::cta_scratch_needed(elem, cap, count, wsm);
             CUDA_TRY(h, h->scratch.ensure(need));
             if (adaptive)  // the candidate bit vectors of the slots start cleared
                 CUDA_TRY(h, cudaMemsetAsync(h->scratch.p, 0, need, st));

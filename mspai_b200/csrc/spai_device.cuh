@@ -12,6 +12,44 @@
 
 namespace mspai {
 
+// Optional per-phase cycle counters (profiling builds only: -DMSPAI_PHASE_TIMERS).
+#ifdef MSPAI_PHASE_TIMERS
+static __device__ unsigned long long g_phase_cycles[16];
+#define PHASE_BEGIN() long long _ph_t = clock64()
+#define PHASE_MARK(k)                                                        \
+    do {                                                                     \
+        if (g.rank() == 0) {                                                 \
+            const long long _now = clock64();                                \
+            atomicAdd(&g_phase_cycles[k], static_cast<unsigned long long>(_now - _ph_t)); \
+            _ph_t = _now;                                                    \
+        }                                                                    \
+    } while (0)
+// sub-phases inside a phase, counted separately in slots 8..15
+#define SUBPHASE_BEGIN() long long _sph_t = clock64()
+#define SUBPHASE_MARK(k)                                                     \
+    do {                                                                     \
+        if (g.rank() == 0) {                                                 \
+            const long long _now = clock64();                                \
+            atomicAdd(&g_phase_cycles[k], static_cast<unsigned long long>(_now - _sph_t)); \
+            _sph_t = _now;                                                   \
+        }                                                                    \
+    } while (0)
+#else
+#define SUBPHASE_BEGIN() \
+    do {                 \
+    } while (0)
+#define SUBPHASE_MARK(k) \
+    do {                 \
+    } while (0)
+#define PHASE_BEGIN() \
+    do {              \
+    } while (0)
+#define PHASE_MARK(k) \
+    do {              \
+    } while (0)
+#endif
+
+
 constexpr int kEntryBits = 24;  // sort key = (row << 24) | entry index
 constexpr uint64_t kEntryMask = (uint64_t(1) << kEntryBits) - 1;
 constexpr int kMaxEntries = 1 << kEntryBits;

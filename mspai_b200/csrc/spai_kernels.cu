@@ -113,10 +113,11 @@ __global__ void __launch_bounds__(kWarpKernelThreads)
     }
 }
 
-// 128-thread CTAs are bounded to 128 registers per thread so that four columns
-// are solved concurrently on every SM.
-template <class T, int NT>
-__global__ void __launch_bounds__(NT, NT == 128 ? 4 : 1)
+// The solver is latency bound: throughput grows with the columns in flight
+// per SM.  MINB CTAs of 128 threads per SM bound the registers per thread
+// (128 for 4, 64 for 8); the shared-memory area per CTA is chosen with it.
+template <class T, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
     cta_solve_kernel(Problem pb, Caps cap, Output out, const int32_t* __restrict__ list, int count,
                      int32_t* __restrict__ counter, char* __restrict__ scratch, size_t slot_bytes,
                      int wfast_elems, int blocked)
@@ -326,25 +327,26 @@ cudaError_t launch_warp_solve(int elem_bytes, const Problem& pb, const Caps& cap
     return launch_warp_t<double>(pb, cap, out, list, count, counter, st, grid_out);
 }
 
-template <class T, int NT>
+template <class T, int NT, int MINB>
 static cudaError_t launch_cta_t(const Problem& pb, const Caps& cap, const Output& out,
                                 const int32_t* list, int count, int32_t* counter, char* scratch,
                                 size_t scratch_bytes, size_t smem, int blocked, cudaStream_t st,
                                 int* grid_out)
 {
     const size_t slot = SlotLayout<T>(cap, false).bytes;
-    cudaError_t e = cudaFuncSetAttribute(cta_solve_kernel<T, NT>,
+    cudaError_t e = cudaFuncSetAttribute(cta_solve_kernel<T, NT, MINB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess)
         return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cta_solve_kernel<T, NT>, NT, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cta_solve_kernel<T, NT, MINB>, NT,
+                                                      smem);
     if (e != cudaSuccess)
         return e;
     if (per_sm < 1)
         return cudaErrorInvalidConfiguration;
-    int grid = std::min(per_sm, 4) * num_sms();
+    int grid = std::min(per_sm, MINB) * num_sms();
     grid = std::max(1, std::min(grid, count));
     const size_t slots_fit = slot > 0 ? scratch_bytes / slot : 0;
     if (slots_fit < 1)
@@ -352,8 +354,8 @@ static cudaError_t launch_cta_t(const Problem& pb, const Caps& cap, const Output
     grid = static_cast<int>(std::min<size_t>(grid, slots_fit));
     *grid_out = grid;
     const int wfast = static_cast<int>(smem / sizeof(T));
-    cta_solve_kernel<T, NT><<<grid, NT, smem, st>>>(pb, cap, out, list, count, counter, scratch,
-                                                    slot, wfast, blocked);
+    cta_solve_kernel<T, NT, MINB><<<grid, NT, smem, st>>>(pb, cap, out, list, count, counter,
+                                                          scratch, slot, wfast, blocked);
     return cudaGetLastError();
 }
 
@@ -362,18 +364,41 @@ cudaError_t launch_cta_solve(int elem_bytes, size_t smem_w_bytes, bool blocked,
                              const int32_t* list, int count, int32_t* counter, char* scratch,
                              size_t scratch_bytes, cudaStream_t st, int* grid_out)
 {
-    if (elem_bytes == 4)
-        return launch_cta_t<float, 128>(pb, cap, out, list, count, counter, scratch,
+    const int per_sm = cta_per_sm(elem_bytes, smem_w_bytes);
+    if (elem_bytes == 4) {
+        if (per_sm == 8)
+            return launch_cta_t<float, 128, 8>(pb, cap, out, list, count, counter, scratch,
+                                               scratch_bytes, smem_w_bytes, blocked ? 1 : 0, st,
+                                               grid_out);
+        if (per_sm == 6)
+            return launch_cta_t<float, 128, 6>(pb, cap, out, list, count, counter, scratch,
+                                               scratch_bytes, smem_w_bytes, blocked ? 1 : 0, st,
+                                               grid_out);
+        return launch_cta_t<float, 128, 4>(pb, cap, out, list, count, counter, scratch,
+                                           scratch_bytes, smem_w_bytes, blocked ? 1 : 0, st,
+                                           grid_out);
+    }
+    return launch_cta_t<double, 128, 4>(pb, cap, out, list, count, counter, scratch,
                                         scratch_bytes, smem_w_bytes, blocked ? 1 : 0, st,
                                         grid_out);
-    return launch_cta_t<double, 128>(pb, cap, out, list, count, counter, scratch, scratch_bytes,
-                                     smem_w_bytes, blocked ? 1 : 0, st, grid_out);
 }
 
-size_t cta_scratch_needed(int elem_bytes, const Caps& cap, int count)
+int cta_per_sm(int elem_bytes, size_t smem_w_bytes)
+{
+    if (elem_bytes != 4)
+        return 4;
+    if (smem_w_bytes <= 24 * 1024)
+        return 8;
+    if (smem_w_bytes <= 32 * 1024)
+        return 6;
+    return 4;
+}
+
+size_t cta_scratch_needed(int elem_bytes, const Caps& cap, int count, size_t smem_w_bytes)
 {
     const size_t slot = cta_slot_bytes(cap, elem_bytes, false);
-    const size_t slots = static_cast<size_t>(std::min(count, 4 * num_sms()));
+    const size_t slots =
+        static_cast<size_t>(std::min(count, cta_per_sm(elem_bytes, smem_w_bytes) * num_sms()));
     return slot * std::max<size_t>(slots, 1);
 }
 

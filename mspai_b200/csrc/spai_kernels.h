@@ -36,7 +36,9 @@ cudaError_t launch_bucket(const int32_t* E, const int32_t* nk, int n, const Buck
 size_t warp_slot_bytes(const Caps& cap, int elem_bytes);
 size_t cta_slot_bytes(const Caps& cap, int elem_bytes, bool w_smem);
 size_t w_bytes(const Caps& cap, int elem_bytes);
-size_t cta_scratch_needed(int elem_bytes, const Caps& cap, int count);
+// CTAs per SM of the solver for this element size and shared-memory area
+int cta_per_sm(int elem_bytes, size_t smem_w_bytes);
+size_t cta_scratch_needed(int elem_bytes, const Caps& cap, int count, size_t smem_w_bytes);
 cudaError_t launch_warp_solve(int elem_bytes, const Problem& pb, const Caps& cap,
                               const Output& out, const int32_t* list, int count, int32_t* counter,
                               cudaStream_t st, int* grid_out);

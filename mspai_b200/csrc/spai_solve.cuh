@@ -32,26 +32,7 @@
 
 namespace mspai {
 
-// Optional per-phase cycle counters (profiling builds only: -DMSPAI_PHASE_TIMERS).
-#ifdef MSPAI_PHASE_TIMERS
-static __device__ unsigned long long g_phase_cycles[16];
-#define PHASE_BEGIN() long long _ph_t = clock64()
-#define PHASE_MARK(k)                                                        \
-    do {                                                                     \
-        if (g.rank() == 0) {                                                 \
-            const long long _now = clock64();                                \
-            atomicAdd(&g_phase_cycles[k], static_cast<unsigned long long>(_now - _ph_t)); \
-            _ph_t = _now;                                                    \
-        }                                                                    \
-    } while (0)
-#else
-#define PHASE_BEGIN() \
-    do {              \
-    } while (0)
-#define PHASE_MARK(k) \
-    do {              \
-    } while (0)
-#endif
+
 
 // Read-only inputs of a setup (device pointers).
 struct Problem {
@@ -174,8 +155,10 @@ struct SlotLayout {
             o_W = o_rhs = 0;
         }
         else {
-            o_W = take(sizeof(T) * static_cast<size_t>(c.mwmax) * c.nmax);
-            o_rhs = take(sizeof(T) * static_cast<size_t>(c.mwmax) * nr);
+            // the dense folded matrix and its right-hand sides, or the
+            // structured QR's shared rows + one panel and [R, Q^T b]
+            o_W = take(sizeof(T) * static_cast<size_t>(c.mwmax + kPanel) * (c.nmax + nr));
+            o_rhs = o_W;
         }
         bytes = align_up<T>(o, 128);
     }
@@ -588,22 +571,33 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
         PHASE_MARK(1);
         const int wcols = n + nrhs;
         const bool w_smem = s.Wfast && mw * wcols <= s.wfast_elems;
+        // W in global memory (CTA groups): the structured blocked QR, which
+        // keeps only the shared rows and one panel of diagonal rows (panels
+        // staged in the shared area); W in shared memory: the dense blocked QR
+        const bool structured = !w_smem && (G::kWarps > 1) && s.bsc != nullptr && s.Wfast &&
+                                (kPanel + S) * kPanel <= s.wfast_elems;
+        const bool blocked = (G::kWarps > 1) && s.bsc != nullptr && (w_smem || structured);
         T* W = w_smem ? s.Wfast : s.W;
-        T* rhs = W + static_cast<size_t>(mw) * n;  // nrhs columns right after W
-        const int ld = mw;
-        // blocked QR for CTA groups (panels staged in the shared area when W
-        // is in global memory and a panel fits there)
-        const bool blocked = (G::kWarps > 1) && s.bsc != nullptr &&
-                             (w_smem || (s.Wfast && mw * kPanel <= s.wfast_elems));
-        for (int i = g.rank(); i < mw * wcols; i += G::kSize)
-            W[i] = T(0);
+        const int ld = structured ? kPanel + S : mw;
+        const int r0 = structured ? kPanel : 0;  // first shared row in W
+        T* rhs = W + static_cast<size_t>(ld) * n;  // nrhs columns right after W
+        if (structured) {
+            for (int i = g.rank(); i < S * wcols; i += G::kSize) {
+                const int c = i / S, r = i - c * S;
+                W[r0 + r + static_cast<size_t>(c) * ld] = T(0);
+            }
+        }
+        else {
+            for (int i = g.rank(); i < mw * wcols; i += G::kSize)
+                W[i] = T(0);
+        }
         g.sync();
         // shared entries
         for (int i = g.rank(); i < E; i += G::kSize) {
             const int e = static_cast<int>(s.keys[i] & kEntryMask);
             const int u = s.pos[e];
             if (s.rstart[u + 1] - s.rstart[u] >= 2) {
-                const int d = s.tmp[u];
+                const int d = r0 + s.tmp[u];
                 W[static_cast<size_t>(s.ejj[e]) * ld + d] = static_cast<T>(s.ev[e]);
                 if (i == s.rstart[u])
                     for (int c = 0; c < nrhs; c++)
@@ -633,10 +627,18 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
                     tb[c] = warp_sum(tb[c]);
             if (lane == 0) {
                 const double nrm = sqrt(sig);
-                W[static_cast<size_t>(jj) * ld + S + jj] = static_cast<T>(nrm);
-                for (int c = 0; c < nrhs; c++)
-                    rhs[S + jj + static_cast<size_t>(c) * ld] =
-                        static_cast<T>(nrm > 0.0 ? tb[c] / nrm : 0.0);
+                if (structured) {
+                    // diagonal rows kept apart: norms and right-hand sides
+                    s.rinv[jj] = nrm;
+                    for (int c = 0; c < nrhs; c++)
+                        s.gv[jj + static_cast<size_t>(c) * n] = nrm > 0.0 ? tb[c] / nrm : 0.0;
+                }
+                else {
+                    W[static_cast<size_t>(jj) * ld + S + jj] = static_cast<T>(nrm);
+                    for (int c = 0; c < nrhs; c++)
+                        rhs[S + jj + static_cast<size_t>(c) * ld] =
+                            static_cast<T>(nrm > 0.0 ? tb[c] / nrm : 0.0);
+                }
             }
         }
         g.sync();
@@ -666,7 +668,31 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
         RView<T> rv{W, ld};
         T* rhs_s = rhs;
         int ldr = ld;  // leading dimension of the right-hand sides
-        if (blocked) {
+        if (structured) {
+            T* Rg = W + static_cast<size_t>(ld) * wcols;  // [R, Q^T b], ld n
+            group_householder_structured<T>(g, W, ld, S, n, nrhs, s.rinv, s.gv, Rg, s.Wfast,
+                                            s.bsc);
+            rv = RView<T>{Rg, n};
+            rhs_s = Rg + static_cast<size_t>(n) * n;
+            ldr = n;
+            if (static_cast<size_t>(n) * (n + 1) / 2 + static_cast<size_t>(n) * nrhs <=
+                static_cast<size_t>(s.wfast_elems)) {
+                // R (packed) and the right-hand sides move to shared memory
+                T* rp = s.Wfast;
+                T* rh = s.Wfast + static_cast<size_t>(n) * (n + 1) / 2;
+                group_pack_r<T>(g, Rg, n, n, rp);
+                for (int t = g.rank(); t < n * nrhs; t += G::kSize)
+                    rh[t] = rhs_s[t];
+                g.sync();
+                rv = RView<T>{rp, 0};
+                rhs_s = rh;
+            }
+            PHASE_MARK(3);
+            for (int c = 0; c < nrhs; c++)
+                sing |= group_back_substitute_blocked<T>(g, rv, n, rhs_s + static_cast<size_t>(c) * ldr,
+                                                         s.x + static_cast<size_t>(c) * n);
+        }
+        else if (blocked) {
             group_householder_blocked<T>(g, W, ld, mw, n, nrhs, w_smem, s.Wfast, s.bsc);
             if (!w_smem && static_cast<size_t>(n) * (n + 1) / 2 + static_cast<size_t>(n) * nrhs <=
                                static_cast<size_t>(s.wfast_elems)) {
@@ -699,8 +725,21 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
         if (g.rank() == 0) {
             const double dn = n, dmw = mw, dm = m, dr = nrhs;
             double* wk = out.work + 3 * static_cast<size_t>(col);
-            wk[0] += 2.0 * dmw * dn * dn - (2.0 / 3.0) * dn * dn * dn + 4.0 * dmw * dn * dr +
-                     2.0 * E * dr;
+            if (structured) {
+                // panels of (nb + S) rows: factorization and trailing update
+                double f = 0.0;
+                for (int c0 = 0; c0 < n; c0 += kPanel) {
+                    const double nb = min(kPanel, n - c0), mp = nb + S;
+                    const double nc = n + nrhs - c0 - nb;
+                    f += 2.0 * mp * nb * nb - (2.0 / 3.0) * nb * nb * nb +
+                         (4.0 * mp * nb - 2.0 * nb * nb) * nc;
+                }
+                wk[0] += f + 2.0 * E * dr;
+            }
+            else {
+                wk[0] += 2.0 * dmw * dn * dn - (2.0 / 3.0) * dn * dn * dn +
+                         4.0 * dmw * dn * dr + 2.0 * E * dr;
+            }
             wk[1] += 2.0 * dm * dn * dn - (2.0 / 3.0) * dn * dn * dn + 4.0 * dm * dn * dr +
                      2.0 * dm * dn * dr;
             wk[2] += 12.0 * E + 16.0 * dn + 8.0 * dm * dr;
