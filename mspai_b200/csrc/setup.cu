@@ -375,6 +375,9 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     pb.ns = adaptive ? prm->ns : 0;
     pb.um = prm->um;
     const bool mixed = prm->prec == MSPAI_PREC_MIXED && prm->batched;
+    // QR updates (-qr > 0) keep and extend each column's factorization across
+    // the pattern steps (batched scalar adaptive setups)
+    pb.qru = (prm->qr > 0 && adaptive && bs == 1 && prm->batched) ? 1 : 0;
     pb.refine = mixed ? std::max(0, prm->refine) : 0;
     const int elem = mixed ? 4 : 8;
 
@@ -501,6 +504,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
                             : 0;
         cap.lcand = adaptive ? mspai::next_pow2(cap.cmax) : 0;
         cap.nbmap = adaptive ? (nprob + 31) / 32 : 0;
+        cap.qru = pb.qru;
         if (static_cast<int64_t>(cap.emax) >= mspai::kMaxEntries)
             return set_err(h, MSPAI_ERR_CAPACITY, "a column touches %d entries of C (max %d)",
                            cap.emax, mspai::kMaxEntries - 1);

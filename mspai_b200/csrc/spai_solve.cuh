@@ -53,6 +53,7 @@ struct Problem {
     double ep;
     int mn, ns, um, refine;
     int bs;                                  // block size (1: scalar SPAI)
+    int qru;                                 // 1: QR updates across pattern steps
 };
 
 // Results.  Column k's indices/values go to [optr[k], optr[k+1]).
@@ -79,6 +80,7 @@ struct Caps {
     int lcand;     // next_pow2(cmax)
     int nrhs;      // right-hand sides (the block size)
     int nbmap;     // words of the candidate bit vector (adaptive; 0 otherwise)
+    int qru;       // 1: room for the QR-update state (dense W, row/column maps)
 };
 
 // Pointers of one problem slot's workspace.
@@ -105,6 +107,14 @@ struct Slot {
     double* rinv;      // nmax  1 / R(j, j) in FP64
     double* rs;        // (emax / 2 + 1) * nrhs  residual on the shared rows
     int32_t* srow;     // emax / 2 + 1  position in I of each shared row
+    // QR-update state (cap.qru): W columns in the order they joined J, W rows
+    // in the order their rows joined I
+    int32_t* qcol;     // nmax  column of C of each W column
+    int32_t* qpos;     // nmax  its position in the sorted J
+    int32_t* qrow;     // emax  rows of I (sorted) ...
+    int32_t* qwr;      // emax  ... and their W rows, from the previous step
+    int32_t* qwu;      // emax  W row of each position of the current I
+    double* qperm;     // nmax  vectors in W's column order
     int32_t* cand;     // lcand candidate column indices (adaptive)
     int32_t* ctmp;     // cmax + 1 candidate flags / scan
     uint32_t* bmap;    // nbmap words: bit vector over problem columns (adaptive)
@@ -121,7 +131,8 @@ __host__ __device__ inline size_t align_up(size_t v, size_t a)
 template <class T>
 struct SlotLayout {
     size_t o_J, o_off, o_ejj, o_ev, o_pos, o_keys, o_I, o_rstart, o_tmp, o_r, o_W, o_rhs, o_x,
-        o_gv, o_rinv, o_rs, o_srow, o_cand, o_ctmp, o_rho, o_bmap, bytes;
+        o_gv, o_rinv, o_rs, o_srow, o_qcol, o_qpos, o_qrow, o_qwr, o_qwu, o_qperm, o_cand, o_ctmp,
+        o_rho, o_bmap, bytes;
     __host__ __device__ SlotLayout(const Caps& c, bool w_external)
     {
         size_t o = 0;
@@ -140,6 +151,13 @@ struct SlotLayout {
         o_rinv = take(sizeof(double) * c.nmax);
         o_rs = take(sizeof(double) * static_cast<size_t>(c.emax / 2 + 1) * nr);
         o_srow = take(sizeof(int32_t) * (c.emax / 2 + 1));
+        const size_t qn = c.qru ? c.nmax : 1, qe = c.qru ? c.emax : 1;
+        o_qcol = take(sizeof(int32_t) * qn);
+        o_qpos = take(sizeof(int32_t) * qn);
+        o_qrow = take(sizeof(int32_t) * qe);
+        o_qwr = take(sizeof(int32_t) * qe);
+        o_qwu = take(sizeof(int32_t) * qe);
+        o_qperm = take(sizeof(double) * qn);
         o_rho = take(sizeof(double) * (c.cmax > 0 ? c.cmax : 1));
         o_J = take(sizeof(int32_t) * c.nmax);
         o_off = take(sizeof(int32_t) * (c.nmax + 1));
@@ -157,7 +175,13 @@ struct SlotLayout {
         else {
             // the dense folded matrix and its right-hand sides, or the
             // structured QR's shared rows + one panel and [R, Q^T b]
-            o_W = take(sizeof(T) * static_cast<size_t>(c.mwmax + kPanel) * (c.nmax + nr));
+            // (QR updates: the dense C(I,J) with ld emax, nmax + 2 columns)
+            size_t wel = static_cast<size_t>(c.mwmax + kPanel) * (c.nmax + nr);
+            if (c.qru) {
+                const size_t q = static_cast<size_t>(c.emax) * (c.nmax + 2);
+                wel = q > wel ? q : wel;
+            }
+            o_W = take(sizeof(T) * wel);
             o_rhs = o_W;
         }
         bytes = align_up<T>(o, 128);
@@ -180,6 +204,12 @@ struct SlotLayout {
         s.rinv = reinterpret_cast<double*>(base + o_rinv);
         s.rs = reinterpret_cast<double*>(base + o_rs);
         s.srow = reinterpret_cast<int32_t*>(base + o_srow);
+        s.qcol = reinterpret_cast<int32_t*>(base + o_qcol);
+        s.qpos = reinterpret_cast<int32_t*>(base + o_qpos);
+        s.qrow = reinterpret_cast<int32_t*>(base + o_qrow);
+        s.qwr = reinterpret_cast<int32_t*>(base + o_qwr);
+        s.qwu = reinterpret_cast<int32_t*>(base + o_qwu);
+        s.qperm = reinterpret_cast<double*>(base + o_qperm);
         s.cand = reinterpret_cast<int32_t*>(base + o_cand);
         s.ctmp = reinterpret_cast<int32_t*>(base + o_ctmp);
         s.bmap = reinterpret_cast<uint32_t*>(base + o_bmap);
@@ -363,6 +393,165 @@ __device__ double group_residual(const G& g, const Problem& pb, int col, const u
     return g.sum(part);
 }
 
+// Householder QR of columns k0 .. n-1 of W (rows k0 .. m-1 of the trailing
+// block; columns < k0 are already factored), LAPACK dlarfg convention,
+// applied to the later columns and to the extra column `rhs`; tau[k] is kept
+// (0: H = I) so that the reflectors can be applied to columns added later.
+template <class T, class G>
+__device__ void group_householder_from(const G& g, T* W, int ld, int m, int k0, int n, T* rhs,
+                                       double* tau)
+{
+    const int lane = g.lane();
+    const int kmax = min(m, n);
+    for (int k = k0; k < kmax; k++) {
+        T* wk = W + static_cast<size_t>(k) * ld;
+        T part = 0;
+        for (int i = k + 1 + g.rank(); i < m; i += G::kSize)
+            part += wk[i] * wk[i];
+        const T xnorm2 = g.sum(part);
+        if (xnorm2 == T(0)) {
+            if (g.rank() == 0)
+                tau[k] = 0.0;
+            g.sync();
+            continue;
+        }
+        const T alpha = wk[k];
+        const T beta = -copysign(tsqrt<T>(alpha * alpha + xnorm2), alpha);
+        const T tk = (beta - alpha) / beta;
+        const T scale = T(1) / (alpha - beta);
+        g.sync();
+        if (g.rank() == 0) {
+            wk[k] = beta;
+            tau[k] = static_cast<double>(tk);
+        }
+        for (int i = k + 1 + g.rank(); i < m; i += G::kSize)
+            wk[i] *= scale;
+        g.sync();
+        for (int c = k + 1 + g.warp(); c <= n; c += G::kWarps) {
+            T* col = c < n ? W + static_cast<size_t>(c) * ld : rhs;
+            T d = (lane == 0) ? col[k] : T(0);
+            for (int i = k + 1 + lane; i < m; i += 32)
+                d += wk[i] * col[i];
+            d = warp_sum(d) * tk;
+            if (lane == 0)
+                col[k] -= d;
+            for (int i = k + 1 + lane; i < m; i += 32)
+                col[i] -= d * wk[i];
+        }
+        g.sync();
+    }
+}
+
+// One least-squares solve of the QR-update algorithm (the reference's
+// Spai_QRUpdate::SPAI_Column with QR_Update, src/Spai_QRUpdate.imp:33-215,
+// 341-377, qrupdates.cpp:164-327): the factorization of the previous pattern
+// step is kept and extended instead of recomputed.
+//
+// W (ld emax, dense C(I,J), unfolded) holds its columns in the order they
+// joined J (qcol) and its rows in the order they joined I.  The columns of
+// the previous step are factored (reflectors below the diagonal, tau); a
+// step adds the new rows at the bottom (zero in the old columns, so the old
+// reflectors leave them alone) and the new columns at the right, applies the
+// old reflectors to the new columns, factors the new columns below row
+// n_old, and back-substitutes with R in W's column order.  Q^T b lives in
+// column nmax + 1: its new rows get b's raw values.  x comes back in the
+// sorted order of J (qpos).  Returns 1 (uniformly) if R is singular.
+template <class T, class G>
+__device__ int qr_update_solve(const G& g, const Problem& pb, const Caps& cap, Slot<T>& s, int col,
+                               int m, int n, int& m_old, int& n_old)
+{
+    const int lane = g.lane();
+    T* W = s.W;
+    const int ld = cap.emax;
+    T* qb = W + static_cast<size_t>(cap.nmax + 1) * ld;
+    // W rows of the current I: old rows keep theirs, new rows follow in
+    // sorted order
+    for (int u = g.rank(); u < m; u += G::kSize) {
+        const int row = s.I[u];
+        const int q = lower_bound_i32(s.qrow, m_old, row);
+        const bool old = q < m_old && s.qrow[q] == row;
+        s.qwu[u] = old ? s.qwr[q] : -1;
+        s.tmp[u] = old ? 0 : 1;
+    }
+    g.sync();
+    group_exclusive_scan(g, s.tmp, m);
+    for (int u = g.rank(); u < m; u += G::kSize) {
+        if (s.qwu[u] < 0)
+            s.qwu[u] = m_old + s.tmp[u];
+        s.qrow[u] = s.I[u];
+    }
+    g.sync();
+    for (int u = g.rank(); u < m; u += G::kSize)
+        s.qwr[u] = s.qwu[u];
+    // columns: the first step takes J as it is; later steps appended theirs
+    // to qcol in the pattern update
+    for (int t = g.rank(); t < n; t += G::kSize) {
+        if (n_old == 0)
+            s.qcol[t] = s.J[t];
+        s.qpos[t] = lower_bound_i32(s.J, n, n_old == 0 ? s.J[t] : s.qcol[t]);
+    }
+    g.sync();
+    // new rows of the old columns and of Q^T b; the new columns
+    for (int i = g.rank(); i < (m - m_old) * n_old; i += G::kSize) {
+        const int t = i / (m - m_old), r = m_old + i % (m - m_old);
+        W[r + static_cast<size_t>(t) * ld] = T(0);
+    }
+    for (int i = g.rank(); i < m * (n - n_old); i += G::kSize) {
+        const int t = n_old + i / m, r = i % m;
+        W[r + static_cast<size_t>(t) * ld] = T(0);
+    }
+    for (int u = g.rank(); u < m; u += G::kSize)
+        if (s.qwu[u] >= m_old)
+            qb[s.qwu[u]] = static_cast<T>(target_value(pb, col, s.I[u]));
+    g.sync();
+    for (int t = n_old + g.warp(); t < n; t += G::kWarps) {
+        const int jj = s.qpos[t];
+        T* wc = W + static_cast<size_t>(t) * ld;
+        for (int e = s.off[jj] + lane; e < s.off[jj + 1]; e += 32)
+            wc[s.qwu[s.pos[e]]] = static_cast<T>(s.ev[e]);
+    }
+    g.sync();
+    // the old reflectors on the new columns (a warp per column, in order)
+    for (int t = n_old + g.warp(); t < n; t += G::kWarps) {
+        T* wc = W + static_cast<size_t>(t) * ld;
+        for (int k = 0; k < n_old; k++) {
+            const T tk = static_cast<T>(s.rinv[k]);
+            if (tk == T(0))
+                continue;
+            const T* wk = W + static_cast<size_t>(k) * ld;
+            T d = (lane == 0) ? wc[k] : T(0);
+            for (int i = k + 1 + lane; i < m; i += 32)
+                d += wk[i] * wc[i];
+            d = warp_sum(d) * tk;
+            __syncwarp();
+            if (lane == 0)
+                wc[k] -= d;
+            for (int i = k + 1 + lane; i < m; i += 32)
+                wc[i] -= d * wk[i];
+            __syncwarp();
+        }
+    }
+    g.sync();
+    // factor the new columns below the old R; tau kept in s.rinv
+    group_householder_from<T>(g, W, ld, m, n_old, n, qb, s.rinv);
+    // fewer rows than columns: R has no rows m..n-1 (rank deficient)
+    for (int k = m + g.rank(); k < n; k += G::kSize)
+        W[k + static_cast<size_t>(k) * ld] = T(0);
+    g.sync();
+    // back substitution on a copy of Q^T b (column n is free)
+    T* rhs = W + static_cast<size_t>(n) * ld;
+    for (int i = g.rank(); i < n; i += G::kSize)
+        rhs[i] = qb[i];
+    g.sync();
+    const int sing = group_back_substitute<T>(g, W, ld, n, rhs, s.qperm);
+    for (int t = g.rank(); t < n; t += G::kSize)
+        s.x[s.qpos[t]] = s.qperm[t];
+    g.sync();
+    m_old = m;
+    n_old = n;
+    return sing;
+}
+
 // Fixed-pattern refinement residual: r = b - C(I,J) x in FP64 and the
 // gradient gv = C(I,J)^T r, for the nrhs right-hand sides, in one pass over
 // the entries (no pass over the rows of I).  `code[e]` is -1 for an entry that
@@ -488,6 +677,10 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
     int n = 0;
     auto scol = [&](int jj) { return bs == 1 ? s.J[jj] : bs * s.J[jj / bs] + jj % bs; };
 
+    // QR updates across the pattern steps (CTA groups, scalar, adaptive)
+    const bool qru = pb.qru && cap.qru && bs == 1 && pb.ns > 0 && (G::kWarps > 1);
+    int q_m_old = 0, q_n_old = 0;
+
     PHASE_BEGIN();
     for (int step = -1; step < pb.ns && status != 3; step++) {
         n = nbk * bs;
@@ -570,74 +763,77 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
         }
         PHASE_MARK(1);
         const int wcols = n + nrhs;
-        const bool w_smem = s.Wfast && mw * wcols <= s.wfast_elems;
+        const bool w_smem = !qru && s.Wfast && mw * wcols <= s.wfast_elems;
         // W in global memory (CTA groups): the structured blocked QR, which
         // keeps only the shared rows and one panel of diagonal rows (panels
         // staged in the shared area); W in shared memory: the dense blocked QR
-        const bool structured = !w_smem && (G::kWarps > 1) && s.bsc != nullptr && s.Wfast &&
-                                (kPanel + S) * kPanel <= s.wfast_elems;
-        const bool blocked = (G::kWarps > 1) && s.bsc != nullptr && (w_smem || structured);
+        const bool structured = !qru && !w_smem && (G::kWarps > 1) && s.bsc != nullptr &&
+                                s.Wfast && (kPanel + S) * kPanel <= s.wfast_elems;
+        const bool blocked =
+            !qru && (G::kWarps > 1) && s.bsc != nullptr && (w_smem || structured);
         T* W = w_smem ? s.Wfast : s.W;
-        const int ld = structured ? kPanel + S : mw;
+        const int ld = qru ? cap.emax : (structured ? kPanel + S : mw);
         const int r0 = structured ? kPanel : 0;  // first shared row in W
         T* rhs = W + static_cast<size_t>(ld) * n;  // nrhs columns right after W
-        if (structured) {
-            for (int i = g.rank(); i < S * wcols; i += G::kSize) {
-                const int c = i / S, r = i - c * S;
-                W[r0 + r + static_cast<size_t>(c) * ld] = T(0);
+        if (!qru) {
+            if (structured) {
+                for (int i = g.rank(); i < S * wcols; i += G::kSize) {
+                    const int c = i / S, r = i - c * S;
+                    W[r0 + r + static_cast<size_t>(c) * ld] = T(0);
+                }
             }
-        }
-        else {
-            for (int i = g.rank(); i < mw * wcols; i += G::kSize)
-                W[i] = T(0);
-        }
-        g.sync();
-        // shared entries
-        for (int i = g.rank(); i < E; i += G::kSize) {
-            const int e = static_cast<int>(s.keys[i] & kEntryMask);
-            const int u = s.pos[e];
-            if (s.rstart[u + 1] - s.rstart[u] >= 2) {
-                const int d = r0 + s.tmp[u];
-                W[static_cast<size_t>(s.ejj[e]) * ld + d] = static_cast<T>(s.ev[e]);
-                if (i == s.rstart[u])
-                    for (int c = 0; c < nrhs; c++)
-                        rhs[d + static_cast<size_t>(c) * ld] =
-                            static_cast<T>(target_value(pb, bs * col + c, s.I[u]));
+            else {
+                for (int i = g.rank(); i < mw * wcols; i += G::kSize)
+                    W[i] = T(0);
             }
-        }
-        // singleton rows, folded per column (one warp per column)
-        for (int jj = g.warp(); jj < n; jj += G::kWarps) {
-            double sig = 0.0;
-            double tb[4] = {0.0, 0.0, 0.0, 0.0};
-            for (int e = s.off[jj] + lane; e < s.off[jj + 1]; e += 32) {
+            g.sync();
+            // shared entries
+            for (int i = g.rank(); i < E; i += G::kSize) {
+                const int e = static_cast<int>(s.keys[i] & kEntryMask);
                 const int u = s.pos[e];
-                if (s.rstart[u + 1] - s.rstart[u] == 1) {
-                    const double v = s.ev[e];
-                    sig += v * v;
-#pragma unroll
-                    for (int c = 0; c < 4; c++)
-                        if (c < nrhs)
-                            tb[c] += v * target_value(pb, bs * col + c, s.I[u]);
+                if (s.rstart[u + 1] - s.rstart[u] >= 2) {
+                    const int d = r0 + s.tmp[u];
+                    W[static_cast<size_t>(s.ejj[e]) * ld + d] = static_cast<T>(s.ev[e]);
+                    if (i == s.rstart[u])
+                        for (int c = 0; c < nrhs; c++)
+                            rhs[d + static_cast<size_t>(c) * ld] =
+                                static_cast<T>(target_value(pb, bs * col + c, s.I[u]));
                 }
             }
-            sig = warp_sum(sig);
-#pragma unroll
-            for (int c = 0; c < 4; c++)
-                if (c < nrhs)
-                    tb[c] = warp_sum(tb[c]);
-            if (lane == 0) {
-                const double nrm = sqrt(sig);
-                if (structured) {
-                    // diagonal rows kept apart: norms and right-hand sides
-                    s.rinv[jj] = nrm;
-                    for (int c = 0; c < nrhs; c++)
-                        s.gv[jj + static_cast<size_t>(c) * n] = nrm > 0.0 ? tb[c] / nrm : 0.0;
+            // singleton rows, folded per column (one warp per column)
+            for (int jj = g.warp(); jj < n; jj += G::kWarps) {
+                double sig = 0.0;
+                double tb[4] = {0.0, 0.0, 0.0, 0.0};
+                for (int e = s.off[jj] + lane; e < s.off[jj + 1]; e += 32) {
+                    const int u = s.pos[e];
+                    if (s.rstart[u + 1] - s.rstart[u] == 1) {
+                        const double v = s.ev[e];
+                        sig += v * v;
+    #pragma unroll
+                        for (int c = 0; c < 4; c++)
+                            if (c < nrhs)
+                                tb[c] += v * target_value(pb, bs * col + c, s.I[u]);
+                    }
                 }
-                else {
-                    W[static_cast<size_t>(jj) * ld + S + jj] = static_cast<T>(nrm);
-                    for (int c = 0; c < nrhs; c++)
-                        rhs[S + jj + static_cast<size_t>(c) * ld] =
-                            static_cast<T>(nrm > 0.0 ? tb[c] / nrm : 0.0);
+                sig = warp_sum(sig);
+    #pragma unroll
+                for (int c = 0; c < 4; c++)
+                    if (c < nrhs)
+                        tb[c] = warp_sum(tb[c]);
+                if (lane == 0) {
+                    const double nrm = sqrt(sig);
+                    if (structured) {
+                        // diagonal rows kept apart: norms and right-hand sides
+                        s.rinv[jj] = nrm;
+                        for (int c = 0; c < nrhs; c++)
+                            s.gv[jj + static_cast<size_t>(c) * n] = nrm > 0.0 ? tb[c] / nrm : 0.0;
+                    }
+                    else {
+                        W[static_cast<size_t>(jj) * ld + S + jj] = static_cast<T>(nrm);
+                        for (int c = 0; c < nrhs; c++)
+                            rhs[S + jj + static_cast<size_t>(c) * ld] =
+                                static_cast<T>(nrm > 0.0 ? tb[c] / nrm : 0.0);
+                    }
                 }
             }
         }
@@ -668,7 +864,12 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
         RView<T> rv{W, ld};
         T* rhs_s = rhs;
         int ldr = ld;  // leading dimension of the right-hand sides
-        if (structured) {
+        const int q_n_old_before = q_n_old;
+        if (qru) {
+            sing = qr_update_solve<T>(g, pb, cap, s, col, m, n, q_m_old, q_n_old);
+            PHASE_MARK(3);
+        }
+        else if (structured) {
             T* Rg = W + static_cast<size_t>(ld) * wcols;  // [R, Q^T b], ld n
             group_householder_structured<T>(g, W, ld, S, n, nrhs, s.rinv, s.gv, Rg, s.Wfast,
                                             s.bsc);
@@ -722,10 +923,19 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
         }
         steps++;
         status = sing ? 1 : 0;
+        const int q_n_old_prev = qru ? q_n_old_before : 0;
         if (g.rank() == 0) {
             const double dn = n, dmw = mw, dm = m, dr = nrhs;
             double* wk = out.work + 3 * static_cast<size_t>(col);
-            if (structured) {
+            if (qru) {
+                // the previous columns' reflectors on the new ones, then the
+                // new block below the old R
+                const double dk = q_n_old_prev, dd = dn - dk;
+                wk[0] += 4.0 * dm * dk * dd + 2.0 * (dm - dk) * dd * dd -
+                         (2.0 / 3.0) * dd * dd * dd + 4.0 * (dm - dk) * dd + dn * dn +
+                         2.0 * E * dr;
+            }
+            else if (structured) {
                 // panels of (nb + S) rows: factorization and trailing update
                 double f = 0.0;
                 for (int c0 = 0; c0 < n; c0 += kPanel) {
@@ -795,11 +1005,25 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
                         s.gv[t] = d;
                 }
                 g.sync();
-                for (int c = 0; c < nrhs; c++) {
-                    if (blocked)
-                        group_normal_correction_blocked<T>(g, rv, n, s.gv + static_cast<size_t>(c) * n);
-                    else
-                        group_normal_correction<T>(g, W, ld, n, s.gv + static_cast<size_t>(c) * n);
+                if (qru) {
+                    // R is in W's column order: permute, correct, permute back
+                    for (int t = g.rank(); t < n; t += G::kSize)
+                        s.qperm[t] = s.gv[s.qpos[t]];
+                    g.sync();
+                    group_normal_correction<T>(g, W, ld, n, s.qperm);
+                    for (int t = g.rank(); t < n; t += G::kSize)
+                        s.gv[s.qpos[t]] = s.qperm[t];
+                    g.sync();
+                }
+                else {
+                    for (int c = 0; c < nrhs; c++) {
+                        if (blocked)
+                            group_normal_correction_blocked<T>(g, rv, n,
+                                                               s.gv + static_cast<size_t>(c) * n);
+                        else
+                            group_normal_correction<T>(g, W, ld, n,
+                                                       s.gv + static_cast<size_t>(c) * n);
+                    }
                 }
                 double d2 = 0.0, x2 = 0.0;
                 for (int t = g.rank(); t < n * nrhs; t += G::kSize) {
@@ -1056,6 +1280,8 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
                     break;
                 if (lane == 0) {
                     s.J[nbk + added] = bj;
+                    if (qru)
+                        s.qcol[nbk + added] = bj;  // W's column order
                     s.cand[bt] = -1;
                 }
                 added++;
