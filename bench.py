@@ -49,7 +49,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--n", type=int, default=1_000_000, help="columns per GPU")
+    ap.add_argument("--columns", "--n", dest="n", type=int, default=1_000_000,
+                    help="columns per GPU")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -196,14 +197,27 @@ def dist_setup(args):
     return world, rank, local
 
 
+def rank_seed(rank):
+    """Seed of rank `rank`'s own block of columns (weak scaling: every rank
+    solves a full workload of its own, no data crosses between ranks)."""
+    return BASE_SEED + rank
+
+
 def max_over_ranks(v, world):
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_rate(n_per_rank, ms_local, world):
+    """(slowest rank's ms per step, columns/s of all ranks together)."""
+    ms = max_over_ranks(ms_local, world)
+    return ms, world * n_per_rank / (ms * 1e-3)
 
 
 def barrier(world):
@@ -258,7 +272,7 @@ def bench_ours(args):
 
     world, rank, local = dist_setup(args)
     n = args.n
-    w = W.ragged(n, seed=BASE_SEED + rank)
+    w = W.ragged(n, seed=rank_seed(rank))
     stream = torch.cuda.current_stream()
     h = mb.Handle(local, stream=stream.cuda_stream)
     dA = mb.DeviceCSC.from_scipy(w.A)
@@ -282,8 +296,7 @@ def bench_ours(args):
     barrier(world)
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1) / args.steps
-    ms = max_over_ranks(ms, world)
-    value = world * n / (ms * 1e-3)
+    ms, value = whole_job_rate(n, ms, world)
     st = h.stats()
     res_mixed, _, status_mixed = h.column_info()
     frob_mixed = float(np.sqrt(np.sum(res_mixed ** 2)))

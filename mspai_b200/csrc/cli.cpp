@@ -119,10 +119,6 @@ int main(int argc, char** argv)
         std::fprintf(stderr, "\n\t%s\n", msg);
         return rc;
     }
-    if (prm.bs != 1) {
-        std::fprintf(stderr, "\n\tblock SPAI (-bs %d) is not available in this build\n", prm.bs);
-        return MSPAI_ERR_PARAM;
-    }
     Owned A, Ce, Be, C, B, P, UP, Bfile;
     if ((rc = read_or_die(a_file, A)) != MSPAI_OK)
         return rc;
@@ -148,7 +144,18 @@ int main(int argc, char** argv)
         bv = mspai_matrix_view(&Bfile.m);
         Bptr = &bv;
     }
-    if (!std::strcmp(p_arg, "-1") || !std::strcmp(p_arg, "-2")) {
+    if (prm.bs > 1 && (!std::strcmp(p_arg, "-1") || !std::strcmp(p_arg, "-2"))) {
+        // block start pattern over the n / bs block columns (a pattern file is
+        // read as such a block pattern)
+        rc = mspai_block_pattern_generate(&cv, prm.bs, !std::strcmp(p_arg, "-1") ? 1 : 2, &P.m);
+        if (rc != MSPAI_OK) {
+            std::fprintf(stderr, "\n\tERROR:  block size %d does not divide n = %d\n", prm.bs,
+                         cv.ncols);
+            return rc;
+        }
+        P.set = true;
+    }
+    else if (!std::strcmp(p_arg, "-1") || !std::strcmp(p_arg, "-2")) {
         rc = mspai_pattern_generate(&cv, !std::strcmp(p_arg, "-1") ? 1 : 2, &P.m);
         if (rc != MSPAI_OK)
             return rc;
@@ -161,6 +168,11 @@ int main(int argc, char** argv)
     pv.values = nullptr;
     const mspai_csc* UPptr = nullptr;
     mspai_csc upv{};
+    if (up_arg && prm.bs > 1) {
+        std::fprintf(stderr, "\n\tERROR:  an upper pattern (-up) with -bs %d is not supported\n",
+                     prm.bs);
+        return MSPAI_ERR_PARAM;
+    }
     if (up_arg) {
         if (!std::strcmp(up_arg, "1") || !std::strcmp(up_arg, "2")) {
             rc = mspai_pattern_generate(&cv, up_arg[0] == '1' ? 1 : 2, &UP.m);

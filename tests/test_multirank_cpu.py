@@ -1,0 +1,78 @@
+"""The multi-rank path of bench.py on CPU (gloo, world size 2, 127.0.0.1).
+
+The setup shards by columns: each rank solves its own block of columns (weak
+scaling), so the only cross-rank steps are the barriers around the timed
+region and the max over ranks of the step time.  These run here with the
+gloo backend; the reference arm must print from rank 0 only."""
+import json
+import os
+import socket
+import subprocess
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, out):
+    import datetime
+    import numpy as np
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    import bench
+    from mspai_b200 import workloads as W
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        bench.barrier(world)
+        ms, value = bench.whole_job_rate(1000, 100.0 + 50.0 * rank, world)
+        w = W.ragged(300, seed=bench.rank_seed(rank))
+        out[rank] = (ms, value, float(np.abs(w.A.data).sum()))
+        bench.barrier(world)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_gloo():
+    world = 2
+    port = free_port()
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.start_processes(_worker, args=(world, port, out), nprocs=world, join=True,
+                           start_method="spawn")
+        r = dict(out)
+    assert set(r) == {0, 1}
+    # every rank sees the slowest rank's time and the whole-job rate
+    for rank in (0, 1):
+        assert r[rank][0] == 150.0
+        assert r[rank][1] == pytest.approx(2 * 1000 / 0.150)
+    # the ranks' column blocks differ (distinct seeds)
+    assert r[0][2] != r[1][2]
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_driver")),
+                    reason="the reference driver is built from the reference sources")
+def test_reference_arm_prints_from_rank_zero_only():
+    port = free_port()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes", "1", "--nproc-per-node",
+           "2", "--master-addr", "127.0.0.1", "--master-port", str(port), "bench.py",
+           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1", "--columns",
+           "2000"]
+    env = dict(os.environ, OMP_NUM_THREADS="1")
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+    assert d["e2e"]["h2d_bytes_per_step"] == 0
