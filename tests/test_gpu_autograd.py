@@ -38,11 +38,11 @@ def test_gradcheck_probing(h, kinds, rho):
     C, B = mb.assemble_probing(A, sp.csr_matrix(E.T @ A), Be, rho)
     h.setup(C, P, B=B, options=mb.Options(ns=0, prec="fp64", probing=1, rho=rho))
     M = h.result()
-    assert float(L) == pytest.approx(float(np.sum(column_residuals(C, M, B) ** 2)), rel=1e-10)
+    assert float(L.detach()) == pytest.approx(float(np.sum(column_residuals(C, M, B) ** 2)), rel=1e-10)
 
 
 def test_gradcheck_plain_spai(h):
-    A = W.ragged(60).tocsc()
+    A = W.ragged_matrix(60).tocsc()
     A.sort_indices()
     P = sp.csc_matrix(A != 0, dtype=np.float64)
     a = torch.tensor(A.data, dtype=torch.float64, requires_grad=True)
