@@ -79,6 +79,7 @@ struct mspai_handle {
     DevBuf oidx, oval, olen, res, steps, status, work;
     DevBuf mptr, midx, mval;  // final M
     DevBuf scratch;
+    DevBuf vflag;  // device input checks
     DevBuf rkeys, rslot_rep, rslot_of, rrep;  // reuse table
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t evb[2 * kBuckets] = {};
@@ -247,21 +248,51 @@ static int check_csc(mspai_handle* h, const mspai_csc* m, const char* name, bool
         return set_err(h, MSPAI_ERR_INPUT, "%s: negative size", name);
     if (m->mem != MSPAI_MEM_HOST && m->mem != MSPAI_MEM_DEVICE)
         return set_err(h, MSPAI_ERR_INPUT, "%s: bad memory kind", name);
-    if (m->mem == MSPAI_MEM_HOST) {
-        if (m->colptr[0] != 0 || m->colptr[m->ncols] != m->nnz)
-            return set_err(h, MSPAI_ERR_INPUT, "%s: column pointers do not match nnz", name);
-        for (int c = 0; c < m->ncols; c++) {
-            if (m->colptr[c + 1] < m->colptr[c])
-                return set_err(h, MSPAI_ERR_INPUT, "%s: column pointers decrease", name);
-            for (int64_t p = m->colptr[c]; p < m->colptr[c + 1]; p++) {
-                const int r = m->rowidx[p];
-                if (r < 0 || r >= m->nrows)
-                    return set_err(h, MSPAI_ERR_INPUT, "%s: row index %d out of range in column %d",
-                                   name, r, c);
-                if (p > m->colptr[c] && m->rowidx[p - 1] >= r)
-                    return set_err(h, MSPAI_ERR_INPUT,
-                                   "%s: row indices not sorted/unique in column %d", name, c);
-            }
+    // the structure itself (pointers, row range, sorted unique rows) is
+    // checked on the device after staging, for host and device inputs alike
+    return MSPAI_OK;
+}
+
+// A staged CSC structure to check on the device.
+struct CscCheck {
+    const char* name;
+    const int64_t* ptr;
+    const int32_t* idx;
+    int ncols, nrows;
+    int64_t nnz;
+    bool nonempty;  // every column needs an entry (C: src/Read_mm_Matrix.cpp:745-751)
+};
+
+// Runs the device checks of `k` staged structures and reports the first error
+// of the first failing one with the messages of the host checks.  No kernel
+// that indexes with these structures runs before this returns MSPAI_OK.
+static int validate_on_device(mspai_handle* h, const CscCheck* cs, int k, cudaStream_t st)
+{
+    CUDA_TRY(h, h->vflag.ensure(sizeof(int32_t) * 4 * k));
+    int32_t* vf = h->vflag.as<int32_t>();
+    CUDA_TRY(h, cudaMemsetAsync(vf, 0, sizeof(int32_t) * 4 * k, st));
+    for (int i = 0; i < k; i++)
+        CUDA_TRY(h, mspai::launch_validate_csc(cs[i].ptr, cs[i].idx, cs[i].ncols, cs[i].nrows,
+                                               cs[i].nnz, cs[i].nonempty, vf + 4 * i, st));
+    int32_t hv[4 * 8] = {};
+    CUDA_TRY(h, cudaMemcpyAsync(hv, vf, sizeof(int32_t) * 4 * k, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    for (int i = 0; i < k; i++) {
+        const int kind = hv[4 * i], c = hv[4 * i + 1], r = hv[4 * i + 2];
+        const char* nm = cs[i].name;
+        switch (kind) {
+        case 0: break;
+        case 1:
+            return set_err(h, MSPAI_ERR_INPUT, "%s: column pointers do not match nnz", nm);
+        case 2: return set_err(h, MSPAI_ERR_INPUT, "%s: column pointers decrease", nm);
+        case 3:
+            return set_err(h, MSPAI_ERR_INPUT, "%s: row index %d out of range in column %d", nm,
+                           r, c);
+        case 4:
+            return set_err(h, MSPAI_ERR_INPUT, "%s: row indices not sorted/unique in column %d",
+                           nm, c);
+        default:
+            return set_err(h, MSPAI_ERR_INPUT, "Matrix is singular: column %d of C is empty", c);
         }
     }
     return MSPAI_OK;
@@ -310,13 +341,6 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
         if (UP->ncols != n || UP->nrows != n)
             return set_err(h, MSPAI_ERR_INPUT, "upper pattern must be %d x %d", n, n);
     }
-    // empty columns of C: the reference rejects them (src/Read_mm_Matrix.cpp:745-751)
-    if (C->mem == MSPAI_MEM_HOST) {
-        for (int c = 0; c < n; c++)
-            if (C->colptr[c + 1] == C->colptr[c])
-                return set_err(h, MSPAI_ERR_INPUT,
-                               "Matrix is singular: column %d of C is empty", c);
-    }
     CUDA_TRY(h, cudaSetDevice(h->device));
     cudaStream_t st = h->stream;
     const bool adaptive = prm->ns > 0 && prm->mn > 0;
@@ -341,6 +365,18 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
         CUDA_TRY(h, stage(h->upptr, UP->colptr, n + 1, UP->mem, st, &pb.upptr));
         CUDA_TRY(h, stage(h->upidx, UP->rowidx, UP->nnz, UP->mem, st, &pb.upidx));
     }
+    {
+        CscCheck cs[4];
+        int k = 0;
+        cs[k++] = CscCheck{"C", pb.cptr, pb.cidx, n, C->nrows, C->nnz, true};
+        cs[k++] = CscCheck{"P", pb.pptr, pb.pidx, nprob, nprob, P->nnz, false};
+        if (B)
+            cs[k++] = CscCheck{"B", pb.bptr, pb.bidx, n, C->nrows, B->nnz, false};
+        if (UP)
+            cs[k++] = CscCheck{"UP", pb.upptr, pb.upidx, n, n, UP->nnz, false};
+        if ((rc = validate_on_device(h, cs, k, st)) != MSPAI_OK)
+            return rc;
+    }
     int max_row_nnz = 0, max_col_nnz = 0;
     if (adaptive) {
         std::vector<int64_t> rp;
@@ -348,8 +384,17 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
         if (C_rows) {
             if ((rc = check_csc(h, C_rows, "C_rows", false)) != MSPAI_OK)
                 return rc;
+            if (C_rows->ncols < n || C_rows->nrows != n)
+                return set_err(h, MSPAI_ERR_INPUT, "C_rows must be the %d x (>= %d) CSC of C^T",
+                               n, n);
             CUDA_TRY(h, stage(h->rptr, C_rows->colptr, C_rows->ncols + 1, C_rows->mem, st, &pb.rptr));
             CUDA_TRY(h, stage(h->rcol, C_rows->rowidx, C_rows->nnz, C_rows->mem, st, &pb.rcol));
+            {
+                const CscCheck cr{"C_rows", pb.rptr, pb.rcol, C_rows->ncols, C_rows->nrows,
+                                  C_rows->nnz, false};
+                if ((rc = validate_on_device(h, &cr, 1, st)) != MSPAI_OK)
+                    return rc;
+            }
             CUDA_TRY(h, fetch(rp, C_rows->colptr, C_rows->ncols + 1, C_rows->mem, st));
         }
         else {

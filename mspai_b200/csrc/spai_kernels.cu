@@ -231,6 +231,48 @@ __global__ void max_len_kernel(const int64_t* __restrict__ ptr, int n, int32_t* 
         atomicMax(out, m);
 }
 
+// ------------------------------------------------------------------ input checks
+// First error found in a CSC structure: err[0] = kind (1 pointers do not match
+// nnz, 2 pointers decrease, 3 row out of range, 4 rows not sorted/unique,
+// 5 empty column), err[1] = column, err[2] = row.  Pointers are checked
+// before any entry of their column is read.
+__global__ void validate_csc_kernel(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                    int ncols, int nrows, int64_t nnz, int nonempty,
+                                    int32_t* __restrict__ err)
+{
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    auto report = [&](int kind, int c, int r) {
+        if (atomicCAS(err, 0, kind) == 0) {
+            err[1] = c;
+            err[2] = r;
+        }
+    };
+    if (tid == 0 && (ptr[0] != 0 || ptr[ncols] != nnz))
+        report(1, -1, 0);
+    for (int c = tid; c < ncols; c += gridDim.x * blockDim.x) {
+        const int64_t a = ptr[c], b = ptr[c + 1];
+        if (a < 0 || b > nnz || b < a) {
+            report(b < a ? 2 : 1, c, 0);
+            continue;
+        }
+        if (nonempty && a == b)
+            report(5, c, 0);
+        int prev = -1;
+        for (int64_t p = a; p < b; p++) {
+            const int r = idx[p];
+            if (r < 0 || r >= nrows) {
+                report(3, c, r);
+                break;
+            }
+            if (r <= prev) {
+                report(4, c, r);
+                break;
+            }
+            prev = r;
+        }
+    }
+}
+
 // ------------------------------------------------------------------ launchers
 namespace {
 int g_num_sms = 0;
@@ -246,6 +288,15 @@ int num_sms()
             g_num_sms = 1;
     }
     return g_num_sms;
+}
+
+cudaError_t launch_validate_csc(const int64_t* ptr, const int32_t* idx, int ncols, int nrows,
+                                int64_t nnz, bool nonempty, int32_t* err, cudaStream_t st)
+{
+    const int blocks = std::max(1, std::min((ncols + 255) / 256, num_sms() * 8));
+    validate_csc_kernel<<<blocks, 256, 0, st>>>(ptr, idx, ncols, nrows, nnz, nonempty ? 1 : 0,
+                                                err);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_plan(const int64_t* cptr, const int64_t* pptr, const int32_t* pidx, int nprob,

@@ -26,6 +26,12 @@ struct BucketRule {
     const int32_t* rep;    // reuse table: columns with rep[k] != k are skipped (nullable)
 };
 
+// Checks a CSC structure on the device (pointers, row range, sorted unique
+// rows, optionally no empty column); the first error goes to err[0..2]
+// (kind, column, row), which must start at zero.
+cudaError_t launch_validate_csc(const int64_t* ptr, const int32_t* idx, int ncols, int nrows,
+                                int64_t nnz, bool nonempty, int32_t* err, cudaStream_t st);
+
 // E[k] = entries of C in the (scalar) columns of problem column k, nk[k] =
 // its scalar pattern size (block pattern entries * bs)
 cudaError_t launch_plan(const int64_t* cptr, const int64_t* pptr, const int32_t* pidx, int nprob,
