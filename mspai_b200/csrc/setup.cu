@@ -365,6 +365,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
         CUDA_TRY(h, stage(h->upptr, UP->colptr, n + 1, UP->mem, st, &pb.upptr));
         CUDA_TRY(h, stage(h->upidx, UP->rowidx, UP->nnz, UP->mem, st, &pb.upidx));
     }
+    int check_launches = 0;
     {
         CscCheck cs[4];
         int k = 0;
@@ -376,6 +377,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
             cs[k++] = CscCheck{"UP", pb.upptr, pb.upidx, n, n, UP->nnz, false};
         if ((rc = validate_on_device(h, cs, k, st)) != MSPAI_OK)
             return rc;
+        check_launches = k;
     }
     int max_row_nnz = 0, max_col_nnz = 0;
     if (adaptive) {
@@ -394,6 +396,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
                                   C_rows->nnz, false};
                 if ((rc = validate_on_device(h, &cr, 1, st)) != MSPAI_OK)
                     return rc;
+                check_launches++;
             }
             CUDA_TRY(h, fetch(rp, C_rows->colptr, C_rows->ncols + 1, C_rows->mem, st));
         }
@@ -427,7 +430,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     const int elem = mixed ? 4 : 8;
 
     // ---- time the device part of the setup
-    h->launches = 0;
+    h->launches = check_launches;  // the input checks ran on the device too
     CUDA_TRY(h, cudaEventRecord(h->ev0, st));
 
     // max column nnz of C (growth bound of the entry count)
