@@ -102,6 +102,11 @@ typedef struct {
                          0: the plain per-column path (one CTA per column,
                          FP64, no buckets) -- the throughput baseline         */
     int32_t verbose;  /* -vb                                                   */
+    int32_t col_begin, col_end; /* solve only problem columns [begin, end)
+                         (0, 0: all); M's other columns are left empty or
+                         zero.  Used to shard the columns over several GPUs;
+                         not in the reference (its column ranges come from
+                         the MPI distribution, src/Distribution.cpp:48-71) */
 } mspai_params;
 
 /* Per-setup statistics. */

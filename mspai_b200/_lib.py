@@ -35,7 +35,8 @@ class mspai_params(ctypes.Structure):
                 ("pk", ctypes.c_int32), ("pm", ctypes.c_int32), ("schur", ctypes.c_int32),
                 ("rho", ctypes.c_double), ("bs", ctypes.c_int32), ("target", ctypes.c_int32),
                 ("probing", ctypes.c_int32), ("prec", ctypes.c_int32), ("refine", ctypes.c_int32),
-                ("batched", ctypes.c_int32), ("verbose", ctypes.c_int32)]
+                ("batched", ctypes.c_int32), ("verbose", ctypes.c_int32),
+                ("col_begin", ctypes.c_int32), ("col_end", ctypes.c_int32)]
 
 
 class mspai_stats(ctypes.Structure):

@@ -47,12 +47,14 @@ class Options:
     refine: int = 2
     batched: bool = True
     verbose: int = 0
+    col_begin: int = 0         # solve only columns [col_begin, col_end) (0, 0: all)
+    col_end: int = 0
 
     def to_c(self) -> mspai_params:
         p = mspai_params()
         _lib.load().mspai_default_params(ctypes.byref(p))
         for f in ("ep", "mn", "ns", "um", "hs", "cs", "qr", "ch", "fg", "pk", "pm", "schur",
-                  "rho", "bs", "target", "probing", "refine", "verbose"):
+                  "rho", "bs", "target", "probing", "refine", "verbose", "col_begin", "col_end"):
             setattr(p, f, getattr(self, f))
         p.prec = _lib.PREC_FP64 if self.prec == "fp64" else _lib.PREC_MIXED
         p.batched = 1 if self.batched else 0

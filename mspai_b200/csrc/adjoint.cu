@@ -201,8 +201,8 @@ __device__ void adjoint_column(const G& g, const Problem& pb, const Caps& cap, S
 
 template <int NT>
 __global__ void __launch_bounds__(NT)
-    adjoint_cta_kernel(Problem pb, Caps cap, AdjointIO io, int n, char* scratch, size_t slot_bytes,
-                       int32_t* counter)
+    adjoint_cta_kernel(Problem pb, Caps cap, AdjointIO io, int lo, int hi, char* scratch,
+                       size_t slot_bytes, int32_t* counter)
 {
     __shared__ GroupScratch sc;
     CtaGroup<NT> g{&sc};
@@ -210,18 +210,18 @@ __global__ void __launch_bounds__(NT)
     Slot<double> s = lay.at(scratch + static_cast<size_t>(blockIdx.x) * slot_bytes, nullptr);
     while (true) {
         if (threadIdx.x == 0)
-            sc.i[5] = atomicAdd(counter, 1);
+            sc.i[5] = lo + atomicAdd(counter, 1);
         __syncthreads();
         const int col = sc.i[5];
         __syncthreads();
-        if (col >= n)
+        if (col >= hi)
             break;
         adjoint_column(g, pb, cap, s, io, col);
     }
 }
 
 __global__ void __launch_bounds__(kWarpKernelThreads)
-    adjoint_warp_kernel(Problem pb, Caps cap, AdjointIO io, int n, char* scratch,
+    adjoint_warp_kernel(Problem pb, Caps cap, AdjointIO io, int lo, int hi, char* scratch,
                         size_t slot_bytes, int32_t* counter)
 {
     __shared__ GroupScratch sc[kWarpKernelThreads / 32];
@@ -234,18 +234,19 @@ __global__ void __launch_bounds__(kWarpKernelThreads)
     while (true) {
         int col = 0;
         if (lane == 0)
-            col = atomicAdd(counter, 1);
+            col = lo + atomicAdd(counter, 1);
         col = __shfl_sync(0xffffffffu, col, 0);
-        if (col >= n)
+        if (col >= hi)
             break;
         adjoint_column(g, pb, cap, s, io, col);
     }
 }
 
-cudaError_t launch_adjoint(const Problem& pb, const Caps& cap, const AdjointIO& io, int n,
-                           bool warp, char* scratch, size_t scratch_bytes, int32_t* counter,
-                           cudaStream_t st)
+cudaError_t launch_adjoint(const Problem& pb, const Caps& cap, const AdjointIO& io, int lo,
+                           int hi, bool warp, char* scratch, size_t scratch_bytes,
+                           int32_t* counter, cudaStream_t st)
 {
+    const int n = hi - lo;  // columns of this launch
     const size_t slot = SlotLayout<double>(cap, false).bytes;
     int dev = 0, sms = 1;
     cudaGetDevice(&dev);
@@ -254,13 +255,13 @@ cudaError_t launch_adjoint(const Problem& pb, const Caps& cap, const AdjointIO& 
         const int per_block = kWarpKernelThreads / 32;
         int grid = std::min<int>(sms * 8, (n + per_block - 1) / per_block);
         grid = std::max(1, std::min<int>(grid, static_cast<int>(scratch_bytes / (slot * per_block))));
-        adjoint_warp_kernel<<<grid, kWarpKernelThreads, 0, st>>>(pb, cap, io, n, scratch, slot,
-                                                                 counter);
+        adjoint_warp_kernel<<<grid, kWarpKernelThreads, 0, st>>>(pb, cap, io, lo, hi, scratch,
+                                                                 slot, counter);
     }
     else {
         int grid = std::min(sms * 4, n);
         grid = std::max(1, std::min<int>(grid, static_cast<int>(scratch_bytes / slot)));
-        adjoint_cta_kernel<128><<<grid, 128, 0, st>>>(pb, cap, io, n, scratch, slot, counter);
+        adjoint_cta_kernel<128><<<grid, 128, 0, st>>>(pb, cap, io, lo, hi, scratch, slot, counter);
     }
     return cudaGetLastError();
 }

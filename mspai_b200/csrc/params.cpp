@@ -34,6 +34,8 @@ extern "C" void mspai_default_params(mspai_params* p)
     p->refine = 2;
     p->batched = 1;
     p->verbose = 0;
+    p->col_begin = 0;
+    p->col_end = 0;
 }
 
 static int fail(char* msg, int len, const char* text)

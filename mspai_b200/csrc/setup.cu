@@ -320,6 +320,13 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
                        "block size %d does not divide the %d columns (constant blocks only)", bs,
                        n);
     const int nprob = n / bs;  // problem columns: scalar columns or block columns
+    // column range of this call (sharding over GPUs): [col_lo, col_hi)
+    const int col_lo = prm->col_begin;
+    const int col_hi = prm->col_end > 0 ? prm->col_end : nprob;
+    if (col_lo < 0 || col_hi > nprob || col_lo > col_hi)
+        return set_err(h, MSPAI_ERR_PARAM, "column range [%d, %d) outside [0, %d)", col_lo,
+                       col_hi, nprob);
+    const bool partial = col_lo > 0 || col_hi < nprob;
     if ((rc = check_csc(h, C, "C", true)) != MSPAI_OK)
         return rc;
     if ((rc = check_csc(h, P, "P", false)) != MSPAI_OK)
@@ -475,6 +482,15 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     }
     CUDA_TRY(h, h->oval.ensure(sizeof(double) * std::max<int64_t>(cap_total, 1)));
     out.oval = h->oval.as<double>();
+    if (partial) {
+        // columns outside the range stay empty (zero values, length 0)
+        CUDA_TRY(h, cudaMemsetAsync(h->oval.p, 0, sizeof(double) * std::max<int64_t>(cap_total, 1),
+                                    st));
+        CUDA_TRY(h, cudaMemsetAsync(h->olen.p, 0, sizeof(int32_t) * std::max(n, 1), st));
+        CUDA_TRY(h, cudaMemsetAsync(h->res.p, 0, sizeof(double) * std::max(n, 1), st));
+        CUDA_TRY(h, cudaMemsetAsync(h->steps.p, 0, sizeof(int32_t) * std::max(n, 1), st));
+        CUDA_TRY(h, cudaMemsetAsync(h->status.p, 0, sizeof(int32_t) * std::max(n, 1), st));
+    }
     out.olen = h->olen.as<int32_t>();
     out.res = h->res.as<double>();
     out.steps = h->steps.as<int32_t>();
@@ -490,7 +506,8 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     CUDA_TRY(h, mspai::launch_plan(pb.cptr, pb.pptr, pb.pidx, nprob, bs, h->E.as<int32_t>(),
                                    h->nk.as<int32_t>(), st));
     // ---- reuse of identical problems (-cs / -ch): fixed scalar patterns
-    const bool reuse = (prm->cs > 0 || prm->ch > 0) && !adaptive && bs == 1 && prm->batched;
+    const bool reuse =
+        (prm->cs > 0 || prm->ch > 0) && !adaptive && bs == 1 && prm->batched && !partial;
     int32_t* drep = nullptr;
     if (reuse) {
         const int max_keys = prm->cs > 0 ? prm->cs : nprob;
@@ -513,6 +530,8 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     CUDA_TRY(h, cudaStreamSynchronize(st));  // max_col_nnz is on the host now
     BucketRule rule{};
     rule.rep = drep;
+    rule.lo = col_lo;
+    rule.hi = col_hi;
     rule.single_bucket = prm->batched ? -1 : 2;
     rule.allow_warp = (adaptive || bs > 1) ? 0 : 1;
     rule.warp_emax = 64;
@@ -655,7 +674,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
         CUDA_TRY(h, cudaMemcpy(&nre, dcnt + 21, sizeof(int32_t), cudaMemcpyDeviceToHost));
         h->stats.reused_columns = nre;
     }
-    h->stats.columns = n;
+    h->stats.columns = static_cast<int64_t>(col_hi - col_lo) * bs;
     h->nprob = nprob;
     h->stats.nnz_m = h->nnz_m;
     h->stats.kernel_launches = h->launches;
@@ -814,6 +833,8 @@ extern "C" int mspai_adjoint(mspai_handle* h, const mspai_csc* C, const mspai_cs
         }
     }
     CUDA_TRY(h, cudaMemsetAsync(io.dC, 0, sizeof(double) * C->nnz, st));
+    if (io.dB)  // entries of columns outside the setup's range stay zero
+        CUDA_TRY(h, cudaMemsetAsync(io.dB, 0, sizeof(double) * B->nnz, st));
     CUDA_TRY(h, lossbuf.ensure(sizeof(double) * std::max(n, 1)));
     io.loss = lossbuf.as<double>();
     CUDA_TRY(h, cudaMemsetAsync(io.loss, 0, sizeof(double) * std::max(n, 1), st));
@@ -827,9 +848,14 @@ extern "C" int mspai_adjoint(mspai_handle* h, const mspai_csc* C, const mspai_cs
     h->launches++;
     CUDA_TRY(h, mspai::launch_plan(pb.cptr, pb.pptr, pb.pidx, n, 1, h->E.as<int32_t>(),
                                    h->nk.as<int32_t>(), st));
+    // the columns of the last setup
+    const int alo = h->last_params.col_begin;
+    const int ahi = h->last_params.col_end > 0 ? h->last_params.col_end : n;
     BucketRule rule{};
     rule.single_bucket = 0;
     rule.elem_bytes = 8;
+    rule.lo = alo;
+    rule.hi = ahi;
     h->launches++;
     CUDA_TRY(h, mspai::launch_bucket(h->E.as<int32_t>(), h->nk.as<int32_t>(), n, rule, dcnt,
                                      dcnt + 4, dcnt + 8, h->lists.as<int32_t>(), st));
@@ -849,7 +875,7 @@ extern "C" int mspai_adjoint(mspai_handle* h, const mspai_csc* C, const mspai_cs
     const size_t need = mspai::adjoint_scratch_bytes(cap, n, warp);
     CUDA_TRY(h, h->scratch.ensure(need));
     CUDA_TRY(h, cudaMemsetAsync(dcnt + 20, 0, sizeof(int32_t), st));
-    CUDA_TRY(h, mspai::launch_adjoint(pb, cap, io, n, warp, h->scratch.as<char>(),
+    CUDA_TRY(h, mspai::launch_adjoint(pb, cap, io, alo, ahi, warp, h->scratch.as<char>(),
                                       h->scratch.bytes, dcnt + 20, st));
     std::vector<double> hl(n);
     if (n > 0)

@@ -67,6 +67,8 @@ __global__ void bucket_kernel(const int32_t* __restrict__ E, const int32_t* __re
 {
     for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < n;
          col += gridDim.x * blockDim.x) {
+        if (col < rule.lo || col >= rule.hi)
+            continue;  // outside the requested column range
         if (rule.rep && rule.rep[col] != col)
             continue;  // solved by its representative
         // sizes after at most ns pattern updates

@@ -24,6 +24,7 @@ struct BucketRule {
     int grow_n;            // mn * ns
     int grow_e;            // mn * ns * max column nnz of C
     const int32_t* rep;    // reuse table: columns with rep[k] != k are skipped (nullable)
+    int lo, hi;            // only problem columns [lo, hi) are binned
 };
 
 // Checks a CSC structure on the device (pointers, row range, sorted unique
@@ -90,9 +91,10 @@ struct AdjointIO {
     double* dB;           // nnz(B) or null
     double* loss;         // per column
 };
-cudaError_t launch_adjoint(const Problem& pb, const Caps& cap, const AdjointIO& io, int n,
-                           bool warp, char* scratch, size_t scratch_bytes, int32_t* counter,
-                           cudaStream_t st);
+// columns [lo, hi) of the last setup
+cudaError_t launch_adjoint(const Problem& pb, const Caps& cap, const AdjointIO& io, int lo,
+                           int hi, bool warp, char* scratch, size_t scratch_bytes,
+                           int32_t* counter, cudaStream_t st);
 size_t adjoint_scratch_bytes(const Caps& cap, int n, bool warp);
 
 }  // namespace mspai

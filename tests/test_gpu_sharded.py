@@ -1,0 +1,74 @@
+"""Column ranges of mspai_setup (col_begin, col_end), the unit of the
+multi-GPU sharding (mspai_b200.distributed): the pieces of M solved range by
+range make the full M, and the adjoints of the ranges sum to the full
+adjoint.  Ranges may land columns in other size buckets than the full setup
+does, so values agree within the FP64 tolerance (1e-10 relative)."""
+import numpy as np
+import pytest
+
+import mspai_b200 as mb
+from helpers import max_rel_diff, same_pattern
+from mspai_b200 import distributed as D
+from mspai_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def h():
+    handle = mb.Handle(0)
+    yield handle
+    handle.close()
+
+
+@pytest.mark.parametrize("case", ["ragged", "convdiff"])
+def test_ranges_make_the_full_setup(h, case):
+    if case == "ragged":
+        w = W.ragged(3000)
+        opts = dict(ns=0, prec="fp64")
+    else:
+        w = W.convdiff3d(8)
+        opts = dict(ep=0.4, ns=5, mn=5, prec="fp64")
+    n = w.A.shape[1]
+    h.setup(w.A, w.P, options=mb.Options(**opts))
+    full = h.result()
+    res_full, steps_full, _ = h.column_info()
+    pieces = []
+    ranges = D.balanced_ranges(D.column_work(w.A, w.P), 3)
+    for lo, hi in ranges:
+        h.setup(w.A, w.P, options=mb.Options(col_begin=lo, col_end=hi, **opts))
+        M = h.result()
+        res, steps, _ = h.column_info()
+        assert np.all(steps[:lo] == 0) and np.all(steps[hi:] == 0)
+        assert np.array_equal(steps[lo:hi], steps_full[lo:hi])
+        assert np.allclose(res[lo:hi], res_full[lo:hi], rtol=1e-10, atol=1e-14)
+        assert h.stats()["columns"] == hi - lo
+        pieces.append(D.local_piece(M, lo, hi))
+    M = D.assemble(pieces, n)
+    assert same_pattern(M, full)
+    assert max_rel_diff(M, full) < 1e-10
+
+
+def test_range_adjoints_sum_to_the_full_adjoint(h):
+    w = W.aniso2d_probing(24, kinds=("ones", "alt"), rho=10.0)
+    C, B = mb.assemble_probing(w.A, w.Ce, w.Be, 10.0)
+    opts = dict(ns=0, prec="fp64", probing=1, rho=10.0)
+    h.setup(C, w.P, B=B, options=mb.Options(**opts))
+    dC, dB, L = h.adjoint(C, B)
+    n = w.A.shape[1]
+    sc, sb, sl = np.zeros_like(dC), np.zeros_like(dB), 0.0
+    for lo, hi in ((0, n // 3), (n // 3, n)):
+        h.setup(C, w.P, B=B, options=mb.Options(col_begin=lo, col_end=hi, **opts))
+        a, b, l = h.adjoint(C, B)
+        sc += a
+        sb += b
+        sl += l
+    assert np.allclose(sc, dC, rtol=1e-9, atol=1e-12 * np.abs(dC).max())
+    assert np.allclose(sb, dB, rtol=1e-9, atol=1e-12 * np.abs(dB).max())
+    assert sl == pytest.approx(L, rel=1e-12)
+
+
+def test_invalid_range_is_rejected(h):
+    w = W.poisson2d(8)
+    with pytest.raises(mb.MspaiError, match="range"):
+        h.setup(w.A, w.P, options=mb.Options(ns=0, col_begin=10, col_end=5))

@@ -10,6 +10,7 @@ import socket
 import subprocess
 import sys
 
+import numpy as np
 import pytest
 import torch.multiprocessing as mp
 
@@ -58,6 +59,68 @@ def test_two_ranks_gloo():
         assert r[rank][1] == pytest.approx(2 * 1000 / 0.150)
     # the ranks' column blocks differ (distinct seeds)
     assert r[0][2] != r[1][2]
+
+
+def _shard_worker(rank, world, port, out):
+    import datetime
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from mspai_b200 import distributed as D
+    from mspai_b200 import workloads as W
+    from oracle import pyoracle as O
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))
+    try:
+        w = W.convdiff3d(6)
+        lo, hi = D.shard_range(w.A, w.P, rank, world)
+        # the oracle stands in for this rank's GPU solve of its columns
+        part = O.spai_scalar(w.A, w.P, ep=0.4, ns=5, mn=5, cols=(lo, hi)).M
+        M = D.gather_pieces(D.local_piece(part, lo, hi), w.A.shape[1])
+        out[rank] = (lo, hi, M.indptr.copy(), M.indices.copy(), M.data.copy())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_columns_gather_to_the_full_setup():
+    """Each of two gloo ranks solves its work-balanced column range and the
+    pieces are all-gathered: every rank ends with the whole M."""
+    sys.path.insert(0, ROOT)
+    from mspai_b200 import workloads as W
+    from oracle import pyoracle as O
+    world = 2
+    port = free_port()
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.start_processes(_shard_worker, args=(world, port, out), nprocs=world, join=True,
+                           start_method="spawn")
+        r = dict(out)
+    w = W.convdiff3d(6)
+    full = O.spai_scalar(w.A, w.P, ep=0.4, ns=5, mn=5).M
+    assert r[0][1] == r[1][0] and r[0][0] == 0 and r[1][1] == w.A.shape[1]
+    for rank in (0, 1):
+        _, _, ip, ix, dv = r[rank]
+        assert np.array_equal(ip, full.indptr) and np.array_equal(ix, full.indices)
+        assert np.array_equal(dv, full.data)
+
+
+def test_balanced_ranges():
+    sys.path.insert(0, ROOT)
+    from mspai_b200 import distributed as D
+    from mspai_b200 import workloads as W
+    w = W.ragged(3000)
+    work = D.column_work(w.A, w.P)
+    for world in (1, 2, 3, 8):
+        rs = D.balanced_ranges(work, world)
+        assert rs[0][0] == 0 and rs[-1][1] == len(work)
+        assert all(a[1] == b[0] for a, b in zip(rs, rs[1:]))
+        loads = [work[lo:hi].sum() for lo, hi in rs]
+        assert max(loads) - min(loads) <= 2 * work.max() + 1e-9
+    # a single heavy column: the other ranges may be empty, none overlaps
+    rs = D.balanced_ranges([1.0, 1e9, 1.0], 4)
+    assert rs[0][0] == 0 and rs[-1][1] == 3 and sum(hi - lo for lo, hi in rs) == 3
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_driver")),
