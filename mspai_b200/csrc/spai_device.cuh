@@ -234,6 +234,59 @@ __device__ void group_bitonic_sort(const G& g, K* keys, int L)
     }
 }
 
+// Sorts E distinct keys made of n ascending runs (run r occupies
+// [off[r], off[r + 1])) by merging pairs of runs, ceil(log2 n) rounds.  Each
+// thread writes a contiguous chunk of the output: it finds the pair that holds
+// its first output position, then its split between the pair's two halves by
+// the merge-path binary search (Odeh, Green, Mwassi, Shmueli and Birk, "Merge
+// Path - parallel merging made simple", IPDPSW 2012), and merges sequentially.
+// a and b are two buffers of E keys; returns the one that holds the result.
+template <class K, class G>
+__device__ K* group_merge_runs(const G& g, K* a, K* b, int E, const int* off, int n)
+{
+    const int chunk = (E + G::kSize - 1) / G::kSize;
+    for (int w = 1; w < n; w <<= 1) {
+        const int npairs = (n + 2 * w - 1) / (2 * w);
+        int o = min(E, g.rank() * chunk);
+        const int oe = min(E, o + chunk);
+        while (o < oe) {
+            // the last pair whose output starts at or before o
+            int lo = 0, hi = npairs - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (off[min(2 * mid * w, n)] <= o)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            const int s0 = off[min(2 * lo * w, n)];
+            const int s1 = off[min((2 * lo + 1) * w, n)];
+            const int s2 = off[min((2 * lo + 2) * w, n)];
+            const int la = s1 - s0, lb = s2 - s1, d = o - s0;
+            // keys of the first half among the pair's first d outputs
+            int ilo = max(0, d - lb), ihi = min(d, la);
+            while (ilo < ihi) {
+                const int i = (ilo + ihi) >> 1;
+                if (a[s0 + i] <= a[s1 + d - i - 1])
+                    ilo = i + 1;
+                else
+                    ihi = i;
+            }
+            int ia = s0 + ilo, ib = s1 + (d - ilo);
+            const int end = min(oe, s2);
+            for (; o < end; o++) {
+                const bool take_a = ib >= s2 || (ia < s1 && a[ia] <= a[ib]);
+                b[o] = take_a ? a[ia++] : a[ib++];
+            }
+        }
+        g.sync();
+        K* t = a;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
 __host__ __device__ inline int next_pow2(int v)
 {
     int p = 1;

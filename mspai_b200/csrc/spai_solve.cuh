@@ -698,6 +698,14 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
             break;
         }
         g.sync();
+        // the entries of each column of C are a run sorted by row; with room
+        // for two key buffers and the run offsets in the shared area (free
+        // until W is built) the runs are merged there
+        const size_t merge_bytes = 2 * sizeof(uint64_t) * static_cast<size_t>(E) +
+                                   sizeof(int) * static_cast<size_t>(n + 1);
+        const bool merge = s.Wfast && E > 0 &&
+                           merge_bytes <= static_cast<size_t>(s.wfast_elems) * sizeof(T);
+        uint64_t* kdst = merge ? reinterpret_cast<uint64_t*>(s.Wfast) : s.keys;
         for (int jj = g.warp(); jj < n; jj += G::kWarps) {
             const int j = scol(jj);
             const int64_t base = pb.cptr[j];
@@ -708,28 +716,42 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
                 const int row = pb.cidx[base + t];
                 s.ejj[e] = jj;
                 s.ev[e] = pb.cval[base + t];
-                s.keys[e] = (static_cast<uint64_t>(row) << kEntryBits) | static_cast<uint64_t>(e);
+                kdst[e] = (static_cast<uint64_t>(row) << kEntryBits) | static_cast<uint64_t>(e);
             }
         }
-        const int L = next_pow2(E > 0 ? E : 1);
-        for (int i = E + g.rank(); i < L; i += G::kSize)
-            s.keys[i] = ~uint64_t(0);
-        g.sync();
-        // sort in the CTA's shared area when it fits (it is free until W is
-        // built), else in place in the global slot
-        if (s.Wfast && static_cast<size_t>(L) * sizeof(uint64_t) <=
-                           static_cast<size_t>(s.wfast_elems) * sizeof(T)) {
-            uint64_t* ks = reinterpret_cast<uint64_t*>(s.Wfast);
-            for (int i = g.rank(); i < L; i += G::kSize)
-                ks[i] = s.keys[i];
+        if (merge) {
+            uint64_t* ka = kdst;
+            uint64_t* kb = ka + E;
+            int* offs = reinterpret_cast<int*>(kb + E);
+            for (int i = g.rank(); i <= n; i += G::kSize)
+                offs[i] = s.off[i];
             g.sync();
-            group_bitonic_sort(g, ks, L);
+            const uint64_t* sorted = group_merge_runs(g, ka, kb, E, offs, n);
             for (int i = g.rank(); i < E; i += G::kSize)
-                s.keys[i] = ks[i];
+                s.keys[i] = sorted[i];
             g.sync();
         }
         else {
-            group_bitonic_sort(g, s.keys, L);
+            // bitonic sort of the keys padded to a power of two: in the
+            // shared area when it fits, else in place in the global slot
+            const int L = next_pow2(E > 0 ? E : 1);
+            for (int i = E + g.rank(); i < L; i += G::kSize)
+                s.keys[i] = ~uint64_t(0);
+            g.sync();
+            if (s.Wfast && static_cast<size_t>(L) * sizeof(uint64_t) <=
+                               static_cast<size_t>(s.wfast_elems) * sizeof(T)) {
+                uint64_t* ks = reinterpret_cast<uint64_t*>(s.Wfast);
+                for (int i = g.rank(); i < L; i += G::kSize)
+                    ks[i] = s.keys[i];
+                g.sync();
+                group_bitonic_sort(g, ks, L);
+                for (int i = g.rank(); i < E; i += G::kSize)
+                    s.keys[i] = ks[i];
+                g.sync();
+            }
+            else {
+                group_bitonic_sort(g, s.keys, L);
+            }
         }
 
         PHASE_MARK(0);
