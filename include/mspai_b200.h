@@ -169,6 +169,14 @@ int mspai_result_nnz(mspai_handle* h, int64_t* nnz);
 int mspai_result_copy(mspai_handle* h, int64_t* colptr, int32_t* rowidx, double* values,
                       int32_t mem);
 
+/*
+ * y = M x with the last result M (the preconditioner application of
+ * Apply_MSPAI, src/imspai.cpp:47-53, there a PETSc MatMult): x and y are
+ * vectors of n doubles where `mem` says.  M's columns scatter into y with
+ * FP64 atomics, so y's last bits can vary from call to call.
+ */
+int mspai_apply(mspai_handle* h, const double* x, double* y, int32_t mem);
+
 /* Per column: ||C(I,J) m - b||_2, LS solves, status (arrays of n; host). */
 int mspai_column_info(mspai_handle* h, double* resnorm, int32_t* steps, int32_t* status);
 

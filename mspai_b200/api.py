@@ -207,6 +207,24 @@ class Handle:
         self._check(self._lib.mspai_result_copy(self._h, ptr(colptr), ptr(rowidx), ptr(values),
                                                 MEM_DEVICE if device else MEM_HOST))
 
+    def apply(self, x):
+        """y = M x with the last result (numpy in, numpy out; or a CUDA
+        float64 torch tensor in, one out)."""
+        try:
+            import torch
+            if isinstance(x, torch.Tensor) and x.is_cuda:
+                xt = x.contiguous().to(torch.float64)
+                y = torch.empty_like(xt)
+                self._check(self._lib.mspai_apply(self._h, ctypes.c_void_p(xt.data_ptr()),
+                                                  ctypes.c_void_p(y.data_ptr()), MEM_DEVICE))
+                return y
+        except ImportError:
+            pass
+        xa = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty_like(xa)
+        self._check(self._lib.mspai_apply(self._h, xa.ctypes.data, y.ctypes.data, MEM_HOST))
+        return y
+
     def column_info(self) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
         res = np.zeros(self.n, dtype=np.float64)
         steps = np.zeros(self.n, dtype=np.int32)

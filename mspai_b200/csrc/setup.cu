@@ -80,6 +80,7 @@ struct mspai_handle {
     DevBuf mptr, midx, mval;  // final M
     DevBuf scratch;
     DevBuf vflag;  // device input checks
+    DevBuf ax, ay; // host vectors of mspai_apply
     DevBuf rkeys, rslot_rep, rslot_of, rrep;  // reuse table
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t evb[2 * kBuckets] = {};
@@ -688,6 +689,32 @@ int mspai_result_nnz(mspai_handle* h, int64_t* nnz)
     if (!h || !h->have_result)
         return h ? set_err(h, MSPAI_ERR_STATE, "no setup result") : MSPAI_ERR_STATE;
     *nnz = h->nnz_m;
+    return MSPAI_OK;
+}
+
+int mspai_apply(mspai_handle* h, const double* x, double* y, int32_t mem)
+{
+    if (!h || !h->have_result)
+        return h ? set_err(h, MSPAI_ERR_STATE, "no setup result") : MSPAI_ERR_STATE;
+    if (!x || !y)
+        return set_err(h, MSPAI_ERR_PARAM, "x and y are required");
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    const int n = h->n;
+    const double* dx = x;
+    double* dy = y;
+    if (mem == MSPAI_MEM_HOST) {
+        CUDA_TRY(h, h->ax.ensure(sizeof(double) * std::max(n, 1)));
+        CUDA_TRY(h, h->ay.ensure(sizeof(double) * std::max(n, 1)));
+        CUDA_TRY(h, cudaMemcpyAsync(h->ax.p, x, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+        dx = h->ax.as<double>();
+        dy = h->ay.as<double>();
+    }
+    CUDA_TRY(h, cudaMemsetAsync(dy, 0, sizeof(double) * n, st));
+    CUDA_TRY(h, mspai::launch_csc_spmv(h->res_ptr, h->res_idx, h->res_val, n, dx, dy, st));
+    if (mem == MSPAI_MEM_HOST)
+        CUDA_TRY(h, cudaMemcpyAsync(y, dy, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
     return MSPAI_OK;
 }
 

@@ -27,6 +27,10 @@ struct BucketRule {
     int lo, hi;            // only problem columns [lo, hi) are binned
 };
 
+// y += M x (M n x n CSC on the device, x and y device vectors of n)
+cudaError_t launch_csc_spmv(const int64_t* ptr, const int32_t* idx, const double* val, int n,
+                            const double* x, double* y, cudaStream_t st);
+
 // Checks a CSC structure on the device (pointers, row range, sorted unique
 // rows, optionally no empty column); the first error goes to err[0..2]
 // (kind, column, row), which must start at zero.
