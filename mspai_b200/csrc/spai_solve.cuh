@@ -797,6 +797,25 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
         const int ld = qru ? cap.emax : (structured ? kPanel + S : mw);
         const int r0 = structured ? kPanel : 0;  // first shared row in W
         T* rhs = W + static_cast<size_t>(ld) * n;  // nrhs columns right after W
+        // fixed pattern: per-entry codes, made before W is built (the build
+        // and the refinement read them in entry order); `pos` is not needed
+        // afterwards and takes the codes (-1 or the shared row), the residual
+        // area holds the right-hand side of every singleton entry
+        const bool fixed = (pb.ns == 0);
+        if (fixed) {
+            for (int e = g.rank(); e < E; e += G::kSize) {
+                const int u = s.pos[e];
+                const bool shared = (s.rstart[u + 1] - s.rstart[u]) >= 2;
+                if (!shared)
+                    for (int c = 0; c < nrhs; c++)
+                        s.r[static_cast<size_t>(c) * cap.emax + e] =
+                            target_value(pb, bs * col + c, s.I[u]);
+                s.pos[e] = shared ? s.tmp[u] : -1;
+            }
+            for (int u = g.rank(); u < m; u += G::kSize)
+                if (s.rstart[u + 1] - s.rstart[u] >= 2)
+                    s.srow[s.tmp[u]] = u;
+        }
         if (!qru) {
             if (structured) {
                 for (int i = g.rank(); i < S * wcols; i += G::kSize) {
@@ -810,16 +829,30 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
             }
             g.sync();
             // shared entries
-            for (int i = g.rank(); i < E; i += G::kSize) {
-                const int e = static_cast<int>(s.keys[i] & kEntryMask);
-                const int u = s.pos[e];
-                if (s.rstart[u + 1] - s.rstart[u] >= 2) {
-                    const int d = r0 + s.tmp[u];
-                    W[static_cast<size_t>(s.ejj[e]) * ld + d] = static_cast<T>(s.ev[e]);
-                    if (i == s.rstart[u])
-                        for (int c = 0; c < nrhs; c++)
-                            rhs[d + static_cast<size_t>(c) * ld] =
-                                static_cast<T>(target_value(pb, bs * col + c, s.I[u]));
+            if (fixed) {
+                for (int e = g.rank(); e < E; e += G::kSize) {
+                    const int cd = s.pos[e];
+                    if (cd >= 0)
+                        W[static_cast<size_t>(s.ejj[e]) * ld + r0 + cd] = static_cast<T>(s.ev[e]);
+                }
+                for (int t = g.rank(); t < S * nrhs; t += G::kSize) {
+                    const int c = t / S, d = t - c * S;
+                    rhs[r0 + d + static_cast<size_t>(c) * ld] =
+                        static_cast<T>(target_value(pb, bs * col + c, s.I[s.srow[d]]));
+                }
+            }
+            else {
+                for (int i = g.rank(); i < E; i += G::kSize) {
+                    const int e = static_cast<int>(s.keys[i] & kEntryMask);
+                    const int u = s.pos[e];
+                    if (s.rstart[u + 1] - s.rstart[u] >= 2) {
+                        const int d = r0 + s.tmp[u];
+                        W[static_cast<size_t>(s.ejj[e]) * ld + d] = static_cast<T>(s.ev[e]);
+                        if (i == s.rstart[u])
+                            for (int c = 0; c < nrhs; c++)
+                                rhs[d + static_cast<size_t>(c) * ld] =
+                                    static_cast<T>(target_value(pb, bs * col + c, s.I[u]));
+                    }
                 }
             }
             // singleton rows, folded per column (one warp per column)
@@ -827,18 +860,22 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
                 double sig = 0.0;
                 double tb[4] = {0.0, 0.0, 0.0, 0.0};
                 for (int e = s.off[jj] + lane; e < s.off[jj + 1]; e += 32) {
-                    const int u = s.pos[e];
-                    if (s.rstart[u + 1] - s.rstart[u] == 1) {
+                    int u = 0;
+                    const bool single =
+                        fixed ? s.pos[e] < 0
+                              : (u = s.pos[e], s.rstart[u + 1] - s.rstart[u] == 1);
+                    if (single) {
                         const double v = s.ev[e];
                         sig += v * v;
-    #pragma unroll
+#pragma unroll
                         for (int c = 0; c < 4; c++)
                             if (c < nrhs)
-                                tb[c] += v * target_value(pb, bs * col + c, s.I[u]);
+                                tb[c] += v * (fixed ? s.r[static_cast<size_t>(c) * cap.emax + e]
+                                                    : target_value(pb, bs * col + c, s.I[u]));
                     }
                 }
                 sig = warp_sum(sig);
-    #pragma unroll
+#pragma unroll
                 for (int c = 0; c < 4; c++)
                     if (c < nrhs)
                         tb[c] = warp_sum(tb[c]);
@@ -860,25 +897,6 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
             }
         }
         g.sync();
-        // fixed pattern: per-entry codes for the refinement pass; `pos` is not
-        // needed afterwards and takes the codes (-1 or the shared row), the
-        // residual area holds the right-hand side of every singleton entry
-        const bool fixed = (pb.ns == 0);
-        if (fixed) {
-            for (int e = g.rank(); e < E; e += G::kSize) {
-                const int u = s.pos[e];
-                const bool shared = (s.rstart[u + 1] - s.rstart[u]) >= 2;
-                if (!shared)
-                    for (int c = 0; c < nrhs; c++)
-                        s.r[static_cast<size_t>(c) * cap.emax + e] =
-                            target_value(pb, bs * col + c, s.I[u]);
-                s.pos[e] = shared ? s.tmp[u] : -1;
-            }
-            for (int u = g.rank(); u < m; u += G::kSize)
-                if (s.rstart[u + 1] - s.rstart[u] >= 2)
-                    s.srow[s.tmp[u]] = u;
-            g.sync();
-        }
 
         PHASE_MARK(2);
         // ---- 3. QR, Q^T b, back substitution (per right-hand side)
