@@ -90,7 +90,7 @@ def test_warp_bucket_limits(h):
     P = sp.lil_matrix((n, n))
     for k in range(n):
         for q in range(16):
-            P[(k + q * 3) % n, k] = 1.0
+            P[(k + q * 2) % n, k] = 1.0
     P = sp.csc_matrix(P)
     for prec in ("fp64", "mixed"):
         h.setup(A, P, options=mb.Options(ns=0, prec=prec))
