@@ -170,6 +170,18 @@ int mspai_result_copy(mspai_handle* h, int64_t* colptr, int32_t* rowidx, double*
                       int32_t mem);
 
 /*
+ * Autotuner (the reference has none: its column loop has no launch shape to
+ * pick).  Times setups of problem columns [0, sample_cols) of the given
+ * problem (20000 when sample_cols <= 0) with each candidate shared-memory
+ * area per solver CTA -- 48, 32 and 24 KB, i.e. 4, 6 and 8 CTAs per SM --
+ * keeps the fastest in the handle for its later setups and writes it (KB) to
+ * *smem_kb_out when not NULL.  Leaves the handle without a result.
+ */
+int mspai_tune(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, const mspai_csc* B,
+               const mspai_csc* P, const mspai_csc* UP, const mspai_params* prm,
+               int32_t sample_cols, int32_t* smem_kb_out);
+
+/*
  * y = M x with the last result M (the preconditioner application of
  * Apply_MSPAI, src/imspai.cpp:47-53, there a PETSc MatMult): x and y are
  * vectors of n doubles where `mem` says.  M's columns scatter into y with

@@ -60,7 +60,7 @@ class mspai_matrix(ctypes.Structure):
 # Every symbol the headers declare (checked by the CPU test suite).
 EXPORTED = [
     "mspai_default_params", "mspai_validate_params", "mspai_create", "mspai_setup",
-    "mspai_apply",
+    "mspai_apply", "mspai_tune",
     "mspai_result_nnz", "mspai_result_copy", "mspai_column_info", "mspai_get_stats",
     "mspai_adjoint", "mspai_last_error", "mspai_free", "mspai_version",
     "mspai_matrix_view", "mspai_matrix_free", "mspai_mm_read", "mspai_mm_write",
@@ -94,6 +94,10 @@ def load() -> ctypes.CDLL:
     lib.mspai_result_nnz.restype = I
     lib.mspai_result_copy.argtypes = [V, V, V, V, ctypes.c_int32]
     lib.mspai_result_copy.restype = I
+    lib.mspai_tune.argtypes = [V, P(mspai_csc), P(mspai_csc), P(mspai_csc), P(mspai_csc),
+                               P(mspai_csc), P(mspai_params), ctypes.c_int32,
+                               P(ctypes.c_int32)]
+    lib.mspai_tune.restype = I
     lib.mspai_apply.argtypes = [V, V, V, ctypes.c_int32]
     lib.mspai_apply.restype = I
     lib.mspai_column_info.argtypes = [V, V, V, V]

@@ -183,6 +183,26 @@ class Handle:
         self._check(rc)
         self.n = sc.c.ncols
 
+    def tune(self, C: MatrixLike, P: MatrixLike, B: Optional[MatrixLike] = None,
+             UP: Optional[MatrixLike] = None, C_rows: Optional[MatrixLike] = None,
+             options: Optional[Options] = None, sample_cols: int = 20000) -> int:
+        """Picks the solver's shared-memory area per CTA (KB) by timing setups
+        of a sample of columns (mspai_tune); later setups use it."""
+        opts = options or Options()
+        p = opts.to_c()
+        sc = _Staged(C, False)
+        sp_ = _Staged(P, True)
+        sb = _Staged(B, False) if B is not None else None
+        su = _Staged(UP, True) if UP is not None else None
+        sr = _Staged(C_rows, True) if C_rows is not None else None
+        kb = ctypes.c_int32()
+        rc = self._lib.mspai_tune(self._h, ctypes.byref(sc.c), ctypes.byref(sr.c) if sr else None,
+                                  ctypes.byref(sb.c) if sb else None, ctypes.byref(sp_.c),
+                                  ctypes.byref(su.c) if su else None, ctypes.byref(p),
+                                  int(sample_cols), ctypes.byref(kb))
+        self._check(rc)
+        return int(kb.value)
+
     def nnz(self) -> int:
         v = ctypes.c_int64()
         self._check(self._lib.mspai_result_nnz(self._h, ctypes.byref(v)))

@@ -692,6 +692,44 @@ int mspai_result_nnz(mspai_handle* h, int64_t* nnz)
     return MSPAI_OK;
 }
 
+int mspai_tune(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, const mspai_csc* B,
+               const mspai_csc* P, const mspai_csc* UP, const mspai_params* prm,
+               int32_t sample_cols, int32_t* smem_kb_out)
+{
+    if (!h || !C || !P || !prm)
+        return h ? set_err(h, MSPAI_ERR_PARAM, "C, P and params are required") : MSPAI_ERR_STATE;
+    // candidates: the per-CTA shared-memory area, which sets the CTAs per SM
+    // of the solver (48 KB: 4, 32 KB: 6, 24 KB: 8) and how much of each
+    // column's work (key merge, packed R) stays in shared memory
+    static const int kCandidates[] = {48, 32, 24};
+    const int nprob = P->ncols;
+    const int cols = std::max(1, std::min<int>(sample_cols > 0 ? sample_cols : 20000, nprob));
+    mspai_params q = *prm;
+    q.col_begin = 0;
+    q.col_end = cols;
+    int best = kCandidates[0];
+    double best_ms = 1e300;
+    for (int kb : kCandidates) {
+        h->smem_budget = static_cast<size_t>(kb) * 1024;
+        double ms = 0.0;
+        for (int rep = 0; rep < 2; rep++) {  // the first run warms up
+            const int rc = mspai_setup(h, C, C_rows, B, P, UP, &q);
+            if (rc != MSPAI_OK)
+                return rc;
+            ms = h->stats.setup_ms;
+        }
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = kb;
+        }
+    }
+    h->smem_budget = static_cast<size_t>(best) * 1024;
+    h->have_result = false;  // the sample runs are not a result
+    if (smem_kb_out)
+        *smem_kb_out = best;
+    return MSPAI_OK;
+}
+
 int mspai_apply(mspai_handle* h, const double* x, double* y, int32_t mem)
 {
     if (!h || !h->have_result)

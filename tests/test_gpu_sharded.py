@@ -72,3 +72,18 @@ def test_invalid_range_is_rejected(h):
     w = W.poisson2d(8)
     with pytest.raises(mb.MspaiError, match="range"):
         h.setup(w.A, w.P, options=mb.Options(ns=0, col_begin=10, col_end=5))
+
+
+def test_tuner_picks_a_candidate_and_keeps_results(h):
+    """mspai_tune times column samples under each shared-memory area and keeps
+    the fastest; setups after it give the same M (FP64 tolerance)."""
+    w = W.ragged(20000)
+    h.setup(w.A, w.P, options=mb.Options(ns=0, prec="fp64"))
+    before = h.result()
+    kb = h.tune(w.A, w.P, options=mb.Options(ns=0, prec="fp64"), sample_cols=4000)
+    assert kb in (48, 32, 24)
+    with pytest.raises(mb.MspaiError, match="result"):
+        h.result()  # the sample runs leave no result
+    h.setup(w.A, w.P, options=mb.Options(ns=0, prec="fp64"))
+    after = h.result()
+    assert same_pattern(after, before) and max_rel_diff(after, before) < 1e-10
