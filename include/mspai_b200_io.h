@@ -73,6 +73,20 @@ int mspai_pattern_generate(const mspai_csc* C, int32_t kind, mspai_matrix* P_out
 int mspai_block_pattern_generate(const mspai_csc* C, int32_t bs, int32_t kind,
                                  mspai_matrix* P_out);
 
+/*
+ * Start pattern from the square of A (the first n rows of C), computed on
+ * GPU `device`: P(:, k) = { i : |(A^2)(i, k)| >= drop * max_i |(A^2)(i, k)| }
+ * (drop = 0 keeps the whole pattern of A^2).  The family of the reference's
+ * power patterns (To_Pattern_Powers / To_Pattern_Power,
+ * src/Matrix.imp:359-470, src/Matrix.cpp:602-636, there through PETSc
+ * MatMatMult and a count-based Sparsify); here a relative drop tolerance.
+ * C on the host with values; P_out owned (mspai_matrix_free).  A column of
+ * A^2 may gather at most 8192 products A(i, l) A(l, k), else
+ * MSPAI_ERR_CAPACITY.
+ */
+int mspai_pattern_power2(const mspai_csc* C, double drop, int32_t device, mspai_matrix* P_out,
+                         char* msg, int32_t msg_len);
+
 /* CSR row structure of the first nrows_keep rows of C, as a CSC of C^T. */
 int mspai_row_structure(const mspai_csc* C, int32_t nrows_keep, mspai_matrix* R_out);
 

@@ -66,6 +66,7 @@ EXPORTED = [
     "mspai_matrix_view", "mspai_matrix_free", "mspai_mm_read", "mspai_mm_write",
     "mspai_probing_assemble", "mspai_pattern_generate", "mspai_row_structure",
     "mspai_measure_fma_peak", "mspai_setup_fixed_noalloc", "mspai_block_pattern_generate",
+    "mspai_pattern_power2",
 ]
 
 _lib = None
@@ -137,6 +138,9 @@ def load() -> ctypes.CDLL:
     lib.mspai_block_pattern_generate.argtypes = [P(mspai_csc), ctypes.c_int32, ctypes.c_int32,
                                                  P(mspai_matrix)]
     lib.mspai_block_pattern_generate.restype = I
+    lib.mspai_pattern_power2.argtypes = [P(mspai_csc), ctypes.c_double, ctypes.c_int32,
+                                         P(mspai_matrix), ctypes.c_char_p, ctypes.c_int32]
+    lib.mspai_pattern_power2.restype = I
     lib.mspai_row_structure.argtypes = [P(mspai_csc), ctypes.c_int32, P(mspai_matrix)]
     lib.mspai_row_structure.restype = I
     _lib = lib

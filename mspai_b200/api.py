@@ -368,6 +368,23 @@ def start_pattern(C: sp.spmatrix, kind: Union[int, str]) -> sp.csc_matrix:
         lib.mspai_matrix_free(ctypes.byref(m))
 
 
+def pattern_power2(C: sp.spmatrix, drop: float = 1e-3, device: int = 0) -> sp.csc_matrix:
+    """Start pattern from A^2 on the GPU (mspai_pattern_power2): per column the
+    rows i with |(A^2)(i,k)| >= drop * max_i |(A^2)(i,k)|."""
+    lib = _lib.load()
+    s = _Staged(C, False)
+    m = _lib.mspai_matrix()
+    buf = ctypes.create_string_buffer(512)
+    rc = lib.mspai_pattern_power2(ctypes.byref(s.c), float(drop), int(device), ctypes.byref(m),
+                                  buf, len(buf))
+    if rc != _lib.MSPAI_OK:
+        raise MspaiError(rc, buf.value.decode(errors="replace"))
+    try:
+        return _owned_to_scipy(m)
+    finally:
+        lib.mspai_matrix_free(ctypes.byref(m))
+
+
 def block_pattern(C: sp.spmatrix, bs: int, kind: Union[int, str]) -> sp.csc_matrix:
     """Block start pattern (n/bs x n/bs): -1 / "diag" diagonal blocks, -2 / "A"
     the block pattern of C's first n rows (mspai_block_pattern_generate)."""
