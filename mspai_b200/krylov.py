@@ -21,10 +21,11 @@ Matvec = Callable[[torch.Tensor], torch.Tensor]
 def csr_matvec(A: sp.spmatrix, device="cuda") -> Matvec:
     """x -> A x with A as a torch sparse CSR matrix on the device."""
     A = sp.csr_matrix(A)
+    A.sort_indices()
     At = torch.sparse_csr_tensor(torch.from_numpy(A.indptr.astype(np.int64)),
                                  torch.from_numpy(A.indices.astype(np.int64)),
                                  torch.from_numpy(A.data.astype(np.float64)),
-                                 size=A.shape, device=device)
+                                 size=A.shape, device=device, check_invariants=True)
     return lambda x: torch.mv(At, x)
 
 
