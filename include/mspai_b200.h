@@ -184,8 +184,9 @@ int mspai_tune(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, con
 /*
  * y = M x with the last result M (the preconditioner application of
  * Apply_MSPAI, src/imspai.cpp:47-53, there a PETSc MatMult): x and y are
- * vectors of n doubles where `mem` says.  M's columns scatter into y with
- * FP64 atomics, so y's last bits can vary from call to call.
+ * vectors of n doubles where `mem` says.  The first call after a setup builds
+ * M's row structure on the device; every y_i is then summed over row i in a
+ * fixed order, so repeated calls give bit-identical y.
  */
 int mspai_apply(mspai_handle* h, const double* x, double* y, int32_t mem);
 

@@ -48,10 +48,14 @@ constexpr size_t kNoAllocSlotBytes = size_t(40) << 20;
 static __device__ __align__(256) char g_noalloc_scratch[kNoAllocScratchBytes];
 // [0] work counter, [1] max entries, [2] max |J|, [3] columns over the limits
 static __device__ __align__(16) int g_noalloc_counters[4];
+// first error of the structure checks of C, P and B (4 ints each: kind,
+// column, row, unused), cleared on every call
+static __device__ __align__(16) int g_noalloc_checks[12];
 
 struct DeviceAddrs {
     char* scratch = nullptr;
     int* counters = nullptr;
+    int* checks = nullptr;
     bool ready = false;
 };
 constexpr int kMaxDevices = 64;
@@ -76,6 +80,10 @@ int device_addrs(int device, DeviceAddrs* out)
         if (cudaGetSymbolAddress(&p, g_noalloc_counters) != cudaSuccess)
             return MSPAI_ERR_CUDA;
         a.counters = static_cast<int*>(p);
+        p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_checks) != cudaSuccess)
+            return MSPAI_ERR_CUDA;
+        a.checks = static_cast<int*>(p);
         a.ready = true;
     }
     *out = a;
@@ -208,6 +216,53 @@ extern "C" int mspai_setup_fixed_noalloc(const mspai_csc* C, const mspai_csc* B,
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (n == 0)
         return MSPAI_OK;
+    if (n > kNoAllocMaxColumns)
+        return fail(MSPAI_ERR_CAPACITY, "more columns than the no-allocation limit (1048576)");
+    if (C->nnz < 0 || P->nnz < 0 || (B && B->nnz < 0) || !C->colptr || !P->colptr ||
+        (C->nnz > 0 && (!C->rowidx || !C->values)) || (P->nnz > 0 && !P->rowidx) ||
+        (B && (!B->colptr || (B->nnz > 0 && (!B->rowidx || !B->values)))))
+        return fail(MSPAI_ERR_INPUT, "missing arrays");
+
+    // structure of C, P and B (pointers, row range, sorted unique rows, no empty
+    // column of C), checked before any kernel indexes with them
+    if (cudaMemsetAsync(a.checks, 0, 12 * sizeof(int), st) != cudaSuccess)
+        return fail(MSPAI_ERR_CUDA, "cudaMemsetAsync failed");
+    if (mspai::launch_validate_csc(C->colptr, C->rowidx, n, C->nrows, C->nnz, true, a.checks,
+                                   st) != cudaSuccess ||
+        mspai::launch_validate_csc(P->colptr, P->rowidx, n, n, P->nnz, false, a.checks + 4,
+                                   st) != cudaSuccess ||
+        (B && mspai::launch_validate_csc(B->colptr, B->rowidx, n, C->nrows, B->nnz, false,
+                                         a.checks + 8, st) != cudaSuccess))
+        return fail(MSPAI_ERR_CUDA, "input check launch failed");
+    {
+        int hv[12] = {};
+        if (cudaMemcpyAsync(hv, a.checks, sizeof(hv), cudaMemcpyDeviceToHost, st) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return fail(MSPAI_ERR_CUDA, "input checks failed");
+        static const char* names[3] = {"C", "P", "B"};
+        for (int i = 0; i < 3; i++) {
+            const int kind = hv[4 * i], c = hv[4 * i + 1], r = hv[4 * i + 2];
+            if (kind == 0)
+                continue;
+            char buf[256];
+            switch (kind) {
+            case 1: std::snprintf(buf, sizeof(buf), "%s: column pointers do not match nnz", names[i]); break;
+            case 2: std::snprintf(buf, sizeof(buf), "%s: column pointers decrease", names[i]); break;
+            case 3:
+                std::snprintf(buf, sizeof(buf), "%s: row index %d out of range in column %d",
+                              names[i], r, c);
+                break;
+            case 4:
+                std::snprintf(buf, sizeof(buf), "%s: row indices not sorted/unique in column %d",
+                              names[i], c);
+                break;
+            default:
+                std::snprintf(buf, sizeof(buf), "Matrix is singular: column %d of C is empty", c);
+            }
+            return fail(MSPAI_ERR_INPUT, buf);
+        }
+    }
 
     // sizes (counters start at zero on every call)
     if (cudaMemsetAsync(a.counters, 0, 4 * sizeof(int), st) != cudaSuccess)
@@ -257,8 +312,6 @@ extern "C" int mspai_setup_fixed_noalloc(const mspai_csc* C, const mspai_csc* B,
     cap.lcand = 0;
     cap.nrhs = 1;
     cap.nbmap = 0;
-    if (n > kNoAllocMaxColumns)
-        return fail(MSPAI_ERR_CAPACITY, "more columns than the no-allocation limit (1048576)");
     Output out{};
     out.optr = P->colptr;  // M has P's pattern: only the values are written
     out.oidx = nullptr;
@@ -266,8 +319,10 @@ extern "C" int mspai_setup_fixed_noalloc(const mspai_csc* C, const mspai_csc* B,
     out.oval = values_out;
     out.res = resnorm_out;
     out.status = status_out;
-    // the solver also records |J_k| and the LS-solve count per column; both
-    // are written before the status, so they share the caller's status array
+    // the solver also records |J_k| and the LS-solve count per column.  They
+    // share the caller's status array: solve_column writes a column's length
+    // and step count before its status, from the same thread, in every branch,
+    // so the status is the value that remains
     out.olen = status_out;
     out.steps = status_out;
     // per-column work counters: the array's tail, cleared for this call

@@ -14,6 +14,7 @@
 // the tolerance are counted (pass 1) or written in row order (pass 2, after
 // a scan of the counts).  Up to kMaxProducts products per column.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -188,10 +189,43 @@ extern "C" int mspai_pattern_power2(const mspai_csc* C, double drop, int32_t dev
             std::snprintf(msg, static_cast<size_t>(msg_len), "%s", what);
         return rc;
     };
+    if (!P_out)
+        return fail(MSPAI_ERR_PARAM, "P_out is required");
     std::memset(P_out, 0, sizeof(*P_out));
-    if (!C || C->mem != MSPAI_MEM_HOST || !C->values || drop < 0.0)
-        return fail(MSPAI_ERR_PARAM, "host C with values and drop >= 0 are required");
+    // !(drop >= 0) also refuses a NaN drop tolerance
+    if (!C || C->mem != MSPAI_MEM_HOST || !C->colptr || !(drop >= 0.0) || !std::isfinite(drop) ||
+        (C->nnz > 0 && (!C->values || !C->rowidx)))
+        return fail(MSPAI_ERR_PARAM, "host C with values and a finite drop >= 0 are required");
     const int n = C->ncols;
+    // the kernel assumes a well-formed square-or-taller CSC with sorted rows:
+    // check it here, on the host where the arrays are
+    if (n < 0 || C->nrows < n || C->nnz < 0)
+        return fail(MSPAI_ERR_INPUT, "C must have at least as many rows as columns");
+    if (C->colptr[0] != 0 || C->colptr[n] != C->nnz)
+        return fail(MSPAI_ERR_INPUT, "C: column pointers do not match nnz");
+    for (int k = 0; k < n; k++) {
+        const int64_t a = C->colptr[k], b = C->colptr[k + 1];
+        if (b < a || a < 0 || b > C->nnz) {
+            char buf[128];
+            std::snprintf(buf, sizeof(buf), "C: column pointers decrease at column %d", k);
+            return fail(MSPAI_ERR_INPUT, buf);
+        }
+        int prev = -1;
+        for (int64_t q = a; q < b; q++) {
+            const int r = C->rowidx[q];
+            if (r < 0 || r >= C->nrows) {
+                char buf[128];
+                std::snprintf(buf, sizeof(buf), "C: row index %d out of range in column %d", r, k);
+                return fail(MSPAI_ERR_INPUT, buf);
+            }
+            if (r <= prev) {
+                char buf[128];
+                std::snprintf(buf, sizeof(buf), "C: row indices not sorted/unique in column %d", k);
+                return fail(MSPAI_ERR_INPUT, buf);
+            }
+            prev = r;
+        }
+    }
     if (cudaSetDevice(device) != cudaSuccess)
         return fail(MSPAI_ERR_NO_DEVICE, "no usable CUDA device");
     cudaStream_t st = nullptr;

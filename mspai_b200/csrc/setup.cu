@@ -81,6 +81,9 @@ struct mspai_handle {
     DevBuf scratch;
     DevBuf vflag;  // device input checks
     DevBuf ax, ay; // host vectors of mspai_apply
+    // row structure of the result for mspai_apply (built on first use)
+    DevBuf tptr, tcol, tval, tkeys, tperm0, tperm1, tcnt, ttemp;
+    bool rows_valid = false;
     DevBuf rkeys, rslot_rep, rslot_of, rrep;  // reuse table
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t evb[2 * kBuckets] = {};
@@ -219,7 +222,9 @@ void mspai_free(mspai_handle* h)
                       &h->bval, &h->pptr, &h->pidx, &h->upptr, &h->upidx, &h->E, &h->nk,
                       &h->lists, &h->counters, &h->scan_tmp, &h->cap_len, &h->cap_ptr, &h->oidx,
                       &h->oval, &h->olen, &h->res, &h->steps, &h->status, &h->work, &h->mptr,
-                      &h->midx, &h->mval, &h->scratch};
+                      &h->midx, &h->mval, &h->scratch, &h->vflag, &h->ax, &h->ay,
+                      &h->rkeys, &h->rslot_rep, &h->rslot_of, &h->rrep, &h->tptr, &h->tcol,
+                      &h->tval, &h->tkeys, &h->tperm0, &h->tperm1, &h->tcnt, &h->ttemp};
     for (DevBuf* b : bufs)
         b->release();
     if (h->ev0)
@@ -306,6 +311,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
         return MSPAI_ERR_STATE;
     h->err.clear();
     h->have_result = false;
+    h->rows_valid = false;
     if (!C || !P || !prm)
         return set_err(h, MSPAI_ERR_PARAM, "C, P and params are required");
     char msg[1024];
@@ -314,6 +320,10 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
         return set_err(h, rc, "%s", msg);
     const int n = C->ncols;
     const int bs = prm->bs;
+    if (prm->schur)
+        return set_err(h, MSPAI_ERR_PARAM,
+                       "Schur probing (-schur 1) is not supported by this setup: its target "
+                       "[0; I; rho Be] and the n x N_p pattern are not built");
     if (bs > 4)
         return set_err(h, MSPAI_ERR_PARAM, "block size %d not supported (1..4)", bs);
     if (n % bs != 0)
@@ -748,8 +758,30 @@ int mspai_apply(mspai_handle* h, const double* x, double* y, int32_t mem)
         dx = h->ax.as<double>();
         dy = h->ay.as<double>();
     }
-    CUDA_TRY(h, cudaMemsetAsync(dy, 0, sizeof(double) * n, st));
-    CUDA_TRY(h, mspai::launch_csc_spmv(h->res_ptr, h->res_idx, h->res_val, n, dx, dy, st));
+    if (!h->rows_valid) {
+        const int64_t nnz = h->nnz_m;
+        if (nnz >= (int64_t(1) << 31))
+            return set_err(h, MSPAI_ERR_CAPACITY, "M has too many nonzeros for mspai_apply");
+        const size_t nz = static_cast<size_t>(std::max<int64_t>(nnz, 1));
+        const size_t tb = std::max<size_t>(mspai::rows_build_temp_bytes(nnz, n), 16);
+        CUDA_TRY(h, h->tptr.ensure(sizeof(int64_t) * (n + 1)));
+        CUDA_TRY(h, h->tcol.ensure(sizeof(int32_t) * nz));
+        CUDA_TRY(h, h->tval.ensure(sizeof(double) * nz));
+        CUDA_TRY(h, h->tkeys.ensure(sizeof(int32_t) * nz));
+        CUDA_TRY(h, h->tperm0.ensure(sizeof(int32_t) * nz));
+        CUDA_TRY(h, h->tperm1.ensure(sizeof(int32_t) * nz));
+        CUDA_TRY(h, h->tcnt.ensure(sizeof(int32_t) * std::max(n, 1)));
+        CUDA_TRY(h, h->ttemp.ensure(tb));
+        CUDA_TRY(h, h->scan_tmp.ensure(sizeof(int64_t) * ((n + 1023) / 1024 + 2)));
+        CUDA_TRY(h, mspai::launch_build_rows(
+                        h->res_ptr, h->res_idx, h->res_val, n, n, nnz, h->tptr.as<int64_t>(),
+                        h->tcol.as<int32_t>(), h->tval.as<double>(), h->tkeys.as<int32_t>(),
+                        h->tperm0.as<int32_t>(), h->tperm1.as<int32_t>(), h->tcnt.as<int32_t>(),
+                        h->scan_tmp.as<int64_t>(), h->ttemp.p, h->ttemp.bytes, st));
+        h->rows_valid = true;
+    }
+    CUDA_TRY(h, mspai::launch_csr_gather(h->tptr.as<int64_t>(), h->tcol.as<int32_t>(),
+                                         h->tval.as<double>(), n, dx, dy, st));
     if (mem == MSPAI_MEM_HOST)
         CUDA_TRY(h, cudaMemcpyAsync(y, dy, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(h, cudaStreamSynchronize(st));

@@ -233,24 +233,6 @@ __global__ void max_len_kernel(const int64_t* __restrict__ ptr, int n, int32_t* 
         atomicMax(out, m);
 }
 
-// ------------------------------------------------------------------ applying M
-// y += M x for M in CSC: a warp per column scatters M(:, j) x_j into y with
-// FP64 atomics (the order of the additions into one y_i is not fixed).
-__global__ void csc_spmv_kernel(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                                const double* __restrict__ val, int n,
-                                const double* __restrict__ x, double* __restrict__ y)
-{
-    const int lane = threadIdx.x & 31;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < n; j += warps) {
-        const double xj = x[j];
-        if (xj == 0.0)
-            continue;
-        for (int64_t p = ptr[j] + lane; p < ptr[j + 1]; p += 32)
-            atomicAdd(y + idx[p], val[p] * xj);
-    }
-}
-
 // ------------------------------------------------------------------ input checks
 // First error found in a CSC structure: err[0] = kind (1 pointers do not match
 // nnz, 2 pointers decrease, 3 row out of range, 4 rows not sorted/unique,
@@ -308,16 +290,6 @@ int num_sms()
             g_num_sms = 1;
     }
     return g_num_sms;
-}
-
-cudaError_t launch_csc_spmv(const int64_t* ptr, const int32_t* idx, const double* val, int n,
-                            const double* x, double* y, cudaStream_t st)
-{
-    if (n <= 0)
-        return cudaSuccess;
-    const int blocks = std::max(1, std::min((n + 7) / 8, num_sms() * 16));
-    csc_spmv_kernel<<<blocks, 256, 0, st>>>(ptr, idx, val, n, x, y);
-    return cudaGetLastError();
 }
 
 cudaError_t launch_validate_csc(const int64_t* ptr, const int32_t* idx, int ncols, int nrows,

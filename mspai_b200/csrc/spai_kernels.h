@@ -27,9 +27,18 @@ struct BucketRule {
     int lo, hi;            // only problem columns [lo, hi) are binned
 };
 
-// y += M x (M n x n CSC on the device, x and y device vectors of n)
-cudaError_t launch_csc_spmv(const int64_t* ptr, const int32_t* idx, const double* val, int n,
-                            const double* x, double* y, cudaStream_t st);
+// Row structure (CSR) of a CSC matrix, in ascending column order within each
+// row (apply.cu): tptr nrows + 1, tcol/tval nnz; keys_out, perm_in, perm_out
+// nnz and cnt nrows are scratch; temp of rows_build_temp_bytes(nnz, nrows).
+size_t rows_build_temp_bytes(int64_t nnz, int nrows);
+cudaError_t launch_build_rows(const int64_t* ptr, const int32_t* idx, const double* val,
+                              int ncols, int nrows, int64_t nnz, int64_t* tptr, int32_t* tcol,
+                              double* tval, int32_t* keys_out, int32_t* perm_in, int32_t* perm_out,
+                              int32_t* cnt, int64_t* scan_tmp, void* temp, size_t temp_bytes,
+                              cudaStream_t st);
+// y = M x from M's row structure, a fixed summation order per row
+cudaError_t launch_csr_gather(const int64_t* tptr, const int32_t* tcol, const double* tval,
+                              int nrows, const double* x, double* y, cudaStream_t st);
 
 // Checks a CSC structure on the device (pointers, row range, sorted unique
 // rows, optionally no empty column); the first error goes to err[0..2]

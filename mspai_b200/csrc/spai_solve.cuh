@@ -1360,10 +1360,11 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
         const int64_t ocap = out.optr[sc_col + 1] - o0;
         if (status == 3 || n > ocap) {
             if (g.rank() == 0) {
+                // the status last: a caller may alias olen/steps with status
                 out.olen[sc_col] = 0;
-                out.status[sc_col] = 3;
                 out.res[sc_col] = 0.0;
                 out.steps[sc_col] = steps;
+                out.status[sc_col] = 3;
             }
             continue;
         }

@@ -56,7 +56,7 @@ def run(w, args, name):
 
 def main():
     if not os.path.exists(DRIVER):
-        raise SystemExit("build the reference first: make -C oracle")
+        raise SystemExit("build the reference first: make -C oracle REF=<reference checkout>")
     run(W.poisson2d(16), ["-2", "-1", "-ns", "0"], "poisson2d_16")
     run(W.poisson2d(64), ["-2", "-1", "-ns", "0"], "poisson2d_64")
     adapt = ["-1", "-1", "-ep", "0.4", "-ns", "5", "-mn", "5", "-um", "1"]

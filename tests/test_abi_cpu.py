@@ -121,3 +121,31 @@ def test_no_device_is_reported_without_gpu(has_gpu):
         pytest.skip("a GPU is present")
     with pytest.raises(mb.MspaiError, match="NO_DEVICE"):
         mb.Handle(0)
+
+
+def test_pattern_power2_checks_inputs_on_the_host():
+    """mspai_pattern_power2 refuses malformed host input and a NaN drop before
+    it touches a device (so this runs without a GPU)."""
+    import ctypes
+    from mspai_b200 import _lib
+    lib = _lib.load()
+
+    def call(cp, ri, vv, nrows, drop):
+        c = _lib.mspai_csc(nrows, len(cp) - 1, len(ri), cp.ctypes.data, ri.ctypes.data,
+                           vv.ctypes.data, _lib.MEM_HOST)
+        m = _lib.mspai_matrix()
+        buf = ctypes.create_string_buffer(256)
+        rc = lib.mspai_pattern_power2(ctypes.byref(c), drop, 0, ctypes.byref(m), buf, len(buf))
+        return rc, buf.value.decode()
+
+    cp = np.array([0, 2, 4, 5], dtype=np.int64)
+    vv = np.ones(5)
+    unsorted = np.array([0, 1, 2, 0, 2], dtype=np.int32)  # column 1 lists rows 2, 0
+    rc, msg = call(cp, unsorted, vv, 3, 1e-3)
+    assert rc == 2 and "not sorted" in msg and "column 1" in msg
+    out_of_range = np.array([0, 1, 0, 1, 7], dtype=np.int32)
+    rc, msg = call(cp, out_of_range, vv, 3, 1e-3)
+    assert rc == 2 and "row index 7 out of range in column 2" in msg
+    good = np.array([0, 1, 0, 1, 2], dtype=np.int32)
+    rc, msg = call(cp, good, vv, 3, float("nan"))
+    assert rc == 1 and "drop" in msg

@@ -72,3 +72,31 @@ def test_empty_column_rejected_for_device_inputs_too(h, device):
     with pytest.raises(mb.MspaiError, match="empty"):
         h.setup(raw(A, device), raw(sp.identity(3), device, pattern=True),
                 options=mb.Options(ns=0))
+
+
+def test_schur_probing_is_refused(h):
+    """-schur 1 is refused with a parameter error instead of silently returning
+    the non-Schur M."""
+    w = W.aniso2d_probing(8, kinds=("ones",), rho=1.0)
+    C, B = mb.assemble_probing(w.A, w.Ce, w.Be, 1.0)
+    with pytest.raises(mb.MspaiError, match="Schur"):
+        h.setup(C, w.P, B=B, options=mb.Options(ns=0, probing=1, schur=1))
+    h.setup(w.A, w.P, options=mb.Options(ns=0))  # the handle stays usable
+
+
+@pytest.mark.parametrize("adaptive", [False, True])
+def test_apply_is_deterministic_and_exact(h, adaptive):
+    """y = M x sums each row in a fixed order: repeated calls agree bit for bit
+    (host and device vectors), and y equals the sparse product to rounding."""
+    w = W.ragged(5000) if not adaptive else W.convdiff3d(12)
+    opts = mb.Options(ns=0) if not adaptive else mb.Options(ns=3, mn=3)
+    h.setup(w.A, w.P, options=opts)
+    M = h.result()
+    x = np.random.default_rng(7).standard_normal(w.n)
+    y1 = h.apply(x)
+    y2 = h.apply(x)
+    assert np.array_equal(y1, y2)
+    yd = h.apply(torch.from_numpy(x).cuda()).cpu().numpy()
+    assert np.array_equal(y1, yd)
+    ref = M @ x
+    assert np.max(np.abs(y1 - ref)) <= 1e-13 * max(1.0, np.max(np.abs(ref)))

@@ -87,3 +87,32 @@ def test_refuses_columns_beyond_limits():
     rc, msg, *_ = noalloc(w.A, w.P, None, mb.Options(ns=0, prec="mixed"), torch)
     assert rc == 4, msg  # MSPAI_ERR_CAPACITY
     assert "no-allocation limits" in msg
+
+
+def test_refuses_malformed_pattern_before_indexing():
+    """A row index of P outside [0, n) is reported as an input error by the
+    structure check, which runs before any kernel indexes with P."""
+    torch = pytest.importorskip("torch")
+    w = W.poisson2d(8)
+    n = w.A.shape[1]
+    P = sp.csc_matrix(w.P)
+    P.sort_indices()
+    rows = P.indices.astype(np.int32).copy()
+    rows[P.indptr[3 + 1] - 1] = n + 5  # last row of column 3, out of range (still sorted)
+    lib = _lib.load()
+    dC = mb.DeviceCSC.from_scipy(w.A)
+    dP = mb.DeviceCSC(n, n, torch.from_numpy(P.indptr.astype(np.int64)).cuda(),
+                      torch.from_numpy(rows).cuda(), None)
+    sc, spp = _Staged(dC, False), _Staged(dP, True)
+    vals = torch.zeros(P.nnz, dtype=torch.float64, device="cuda")
+    res = torch.zeros(n, dtype=torch.float64, device="cuda")
+    status = torch.zeros(n, dtype=torch.int32, device="cuda")
+    p = mb.Options(ns=0, prec="mixed").to_c()
+    msg = ctypes.create_string_buffer(512)
+    rc = lib.mspai_setup_fixed_noalloc(ctypes.byref(sc.c), None, ctypes.byref(spp.c),
+                                       ctypes.byref(p), vals.data_ptr(), res.data_ptr(),
+                                       status.data_ptr(), torch.cuda.current_stream().cuda_stream,
+                                       msg, len(msg))
+    torch.cuda.synchronize()
+    assert rc == 2, msg.value  # MSPAI_ERR_INPUT
+    assert "P: row index" in msg.value.decode() and "column 3" in msg.value.decode()
