@@ -321,7 +321,8 @@ def bench_ours(args):
             traffic = None
     roofline = {"bound": "fp32", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
                 "frac": (achieved / peak32) if achieved else None, "traffic": traffic,
-                "kernel": ["warp_solve", "cta_solve(W in smem)", "cta_solve(W in global)"][b],
+                "kernel": ["warp_solve_kernel", "fixed_solve_kernel (first launch)",
+                           "fixed_solve_kernel (large arena)", "cta_solve_kernel (fallback)"][b],
                 "kernel_ms": kms, "flops_per_launch": st["bucket_flops"][b],
                 "peak_source": "measured FP32 FMA probe (mspai_measure_fma_peak)"}
 

@@ -259,10 +259,10 @@ class Handle:
         return {
             "columns": s.columns, "ls_solves": s.ls_solves, "nnz_m": s.nnz_m,
             "singular_columns": s.singular_columns, "capacity_columns": s.capacity_columns,
-            "bucket_columns": list(s.bucket_columns)[:3], "flops": s.flops,
+            "bucket_columns": list(s.bucket_columns), "flops": s.flops,
             "flops_dense": s.flops_dense, "gather_bytes": s.gather_bytes,
-            "setup_ms": s.setup_ms, "kernel_ms": list(s.kernel_ms)[:3],
-            "kernel_launches": s.kernel_launches, "bucket_flops": list(s.bucket_flops)[:3],
+            "setup_ms": s.setup_ms, "kernel_ms": list(s.kernel_ms),
+            "kernel_launches": s.kernel_launches, "bucket_flops": list(s.bucket_flops),
             "reused_columns": s.reused_columns,
         }
 

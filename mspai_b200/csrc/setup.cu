@@ -26,7 +26,12 @@ using mspai::Caps;
 using mspai::Output;
 using mspai::Problem;
 
-constexpr int kBuckets = 3;
+constexpr int kBuckets = 3;    // size buckets of the planning kernel
+constexpr int kKernels = 4;    // solver launches per setup (timed separately)
+constexpr int kLists = 4;      // work lists: buckets + the overflow lists
+// Arena of the fixed-pattern solver's second launch (one CTA per SM): the
+// largest dynamic shared memory a CTA may have beside the solver's static part.
+constexpr int kFixedArenaLarge = 212 * 1024;
 
 // A device buffer that grows on demand.
 struct DevBuf {
@@ -85,8 +90,9 @@ struct mspai_handle {
     DevBuf tptr, tcol, tval, tkeys, tperm0, tperm1, tcnt, ttemp;
     bool rows_valid = false;
     DevBuf rkeys, rslot_rep, rslot_of, rrep;  // reuse table
+    DevBuf rglob;  // per-CTA areas for R of the fixed-pattern solver
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    cudaEvent_t evb[2 * kBuckets] = {};
+    cudaEvent_t evb[2 * kKernels] = {};
     // result description
     int n = 0;
     int64_t nnz_m = 0;
@@ -100,6 +106,10 @@ struct mspai_handle {
     int64_t launches = 0;
     int nprob = 0;  // problem columns of the last setup (n / bs)
     size_t smem_budget = 48 * 1024;  // shared-memory area of each CTA solver (4 per SM)
+    int fixed_arena = 107 * 1024;    // arena of the fixed-pattern solver's first launch (2 CTAs per SM)
+    int fixed_arena_large = kFixedArenaLarge;  // ... and of its second launch
+    bool used_fixed = false;         // the last setup ran the fixed-pattern solver
+    int64_t list_len[kLists] = {};   // columns listed per work list in the last setup
 };
 
 static int set_err(mspai_handle* h, int code, const char* fmt, ...)
@@ -207,6 +217,18 @@ int mspai_create(mspai_handle** out, int32_t device, void* stream)
         if (v >= 16 && v <= 220)
             h->smem_budget = static_cast<size_t>(v) * 1024;
     }
+    // arenas of the fixed-pattern solver's two launches (KB); small values send
+    // columns down the overflow chain (used by the tests of that chain)
+    if (const char* kb = std::getenv("MSPAI_FIXED_ARENA_KB")) {
+        const long v = std::atol(kb);
+        if (v >= 1 && v <= 216)
+            h->fixed_arena = static_cast<int>(v) * 1024;
+    }
+    if (const char* kb = std::getenv("MSPAI_FIXED_ARENA_LARGE_KB")) {
+        const long v = std::atol(kb);
+        if (v >= 1 && v <= 216)
+            h->fixed_arena_large = static_cast<int>(v) * 1024;
+    }
     *out = h;
     return MSPAI_OK;
 }
@@ -224,7 +246,8 @@ void mspai_free(mspai_handle* h)
                       &h->oval, &h->olen, &h->res, &h->steps, &h->status, &h->work, &h->mptr,
                       &h->midx, &h->mval, &h->scratch, &h->vflag, &h->ax, &h->ay,
                       &h->rkeys, &h->rslot_rep, &h->rslot_of, &h->rrep, &h->tptr, &h->tcol,
-                      &h->tval, &h->tkeys, &h->tperm0, &h->tperm1, &h->tcnt, &h->ttemp};
+                      &h->tval, &h->tkeys, &h->tperm0, &h->tperm1, &h->tcnt, &h->ttemp,
+                      &h->rglob};
     for (DevBuf* b : bufs)
         b->release();
     if (h->ev0)
@@ -511,7 +534,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     // ---- plan and bucket
     CUDA_TRY(h, h->E.ensure(sizeof(int32_t) * std::max(nprob, 1)));
     CUDA_TRY(h, h->nk.ensure(sizeof(int32_t) * std::max(nprob, 1)));
-    CUDA_TRY(h, h->lists.ensure(sizeof(int32_t) * static_cast<size_t>(kBuckets) *
+    CUDA_TRY(h, h->lists.ensure(sizeof(int32_t) * static_cast<size_t>(kLists) *
                                 std::max(nprob, 1)));
     h->launches++;
     CUDA_TRY(h, mspai::launch_plan(pb.cptr, pb.pptr, pb.pidx, nprob, bs, h->E.as<int32_t>(),
@@ -547,7 +570,10 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     rule.allow_warp = (adaptive || bs > 1) ? 0 : 1;
     rule.warp_emax = 64;
     rule.warp_nmax = 16;
-    rule.smem_w_bytes = 96 * 1024;
+    // fixed scalar patterns: every column beyond the warp bucket goes to the
+    // fixed-pattern solver (bucket 1), which sizes its arrays per column
+    const bool use_fixed = !adaptive && bs == 1 && prm->batched && !pb.qru;
+    rule.smem_w_bytes = use_fixed ? (int64_t(1) << 62) : 96 * 1024;
     rule.elem_bytes = elem;
     rule.grow_n = grow_n * bs;
     rule.grow_e = adaptive ? grow_n * bs * max_col_nnz : 0;
@@ -560,12 +586,37 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     CUDA_TRY(h, cudaStreamSynchronize(st));
 
     // ---- bucket kernels
-    for (int b = 0; b < kBuckets; b++)
-        h->stats.bucket_columns[b] = hc[b];
-    h->stats.bucket_columns[3] = 0;
+    for (int k = 0; k < kKernels; k++) {
+        h->stats.bucket_columns[k] = 0;
+        h->stats.kernel_ms[k] = 0.0;
+    }
+    for (int k = 0; k < kLists; k++)
+        h->list_len[k] = 0;
+    bool timed[kKernels] = {false, false, false, false};
+    h->used_fixed = use_fixed;
+    // general CTA solver over `count` listed columns with the given caps
+    auto run_cta = [&](int b, const Caps& cap, int32_t* list, int count, int32_t* counter,
+                       size_t wsm_budget) -> int {
+        int grid = 0;
+        size_t wsm = std::min<size_t>(mspai::w_bytes(cap, elem), wsm_budget);
+        if (!prm->batched)
+            wsm = 0;  // the plain path keeps W in global memory, unblocked
+        const size_t need = mspai::cta_scratch_needed(elem, cap, count, wsm);
+        CUDA_TRY(h, h->scratch.ensure(need));
+        if (adaptive)  // the candidate bit vectors of the slots start cleared
+            CUDA_TRY(h, cudaMemsetAsync(h->scratch.p, 0, need, st));
+        CUDA_TRY(h, cudaMemsetAsync(counter, 0, sizeof(int32_t), st));
+        h->launches++;
+        CUDA_TRY(h, mspai::launch_cta_solve(elem, wsm, prm->batched != 0, pb, cap, out, list,
+                                            count, counter, h->scratch.as<char>(),
+                                            h->scratch.bytes, st, &grid));
+        (void)b;
+        return MSPAI_OK;
+    };
     for (int b = 0; b < kBuckets; b++) {
         const int count = hc[b];
-        h->stats.kernel_ms[b] = 0.0;
+        if (!(use_fixed && b == 2))  // with the fixed-pattern solver list 2 is its overflow
+            h->list_len[b] = count;
         if (count == 0)
             continue;
         Caps cap{};
@@ -589,35 +640,71 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
         int32_t* list = h->lists.as<int32_t>() + static_cast<size_t>(b) * nprob;
         int32_t* counter = dcnt + 12 + b;
         CUDA_TRY(h, cudaMemsetAsync(counter, 0, sizeof(int32_t), st));
-        CUDA_TRY(h, cudaEventRecord(h->evb[2 * b], st));
         int grid = 0;
         bool use_warp = (b == 0);
         if (use_warp &&
             mspai::warp_slot_bytes(cap, elem) * (mspai::kWarpKernelThreads / 32) > 200 * 1024)
             use_warp = false;
         if (use_warp) {
+            CUDA_TRY(h, cudaEventRecord(h->evb[0], st));
             h->launches++;
             CUDA_TRY(h, mspai::launch_warp_solve(elem, pb, cap, out, list, count, counter, st,
                                                  &grid));
+            CUDA_TRY(h, cudaEventRecord(h->evb[1], st));
+            timed[0] = true;
+            h->stats.bucket_columns[0] = count;
+        }
+        else if (b == 1 && use_fixed) {
+            // fixed-pattern solver: launch A (tuned arena) over the bucket, its
+            // overflow through launch B (the largest arena), what is left
+            // through the general solver
+            int32_t* ovf_a = h->lists.as<int32_t>() + static_cast<size_t>(2) * nprob;
+            int32_t* ovf_b = h->lists.as<int32_t>() + static_cast<size_t>(3) * nprob;
+            int32_t* cnt = dcnt + 24;  // [0] overflow A, [1] overflow B, [2] queue B
+            CUDA_TRY(h, cudaMemsetAsync(cnt, 0, 3 * sizeof(int32_t), st));
+            const int64_t relems = mspai::fixed_r_elems(cap.nmax);
+            const int grid_max = std::max(mspai::fixed_max_grid(h->fixed_arena),
+                                          mspai::fixed_max_grid(h->fixed_arena_large));
+            CUDA_TRY(h, h->rglob.ensure(static_cast<size_t>(grid_max) * relems * elem));
+            CUDA_TRY(h, cudaEventRecord(h->evb[2], st));
+            h->launches++;
+            CUDA_TRY(h, mspai::launch_fixed_solve(elem, h->fixed_arena, pb, out, list, nullptr,
+                                                  count, counter, ovf_a, cnt, h->rglob.p, relems,
+                                                  grid_max, st, &grid));
+            CUDA_TRY(h, cudaEventRecord(h->evb[3], st));
+            CUDA_TRY(h, cudaEventRecord(h->evb[4], st));
+            h->launches++;
+            CUDA_TRY(h, mspai::launch_fixed_solve(elem, h->fixed_arena_large, pb, out, ovf_a, cnt, 0,
+                                                  cnt + 2, ovf_b, cnt + 1, h->rglob.p, relems,
+                                                  grid_max, st, &grid));
+            CUDA_TRY(h, cudaEventRecord(h->evb[5], st));
+            timed[1] = timed[2] = true;
+            int32_t ho[2] = {0, 0};
+            CUDA_TRY(h, cudaMemcpyAsync(ho, cnt, sizeof(ho), cudaMemcpyDeviceToHost, st));
+            CUDA_TRY(h, cudaStreamSynchronize(st));
+            h->list_len[2] = ho[0];
+            h->list_len[3] = ho[1];
+            h->stats.bucket_columns[1] = count - ho[0];
+            h->stats.bucket_columns[2] = ho[0] - ho[1];
+            h->stats.bucket_columns[3] = ho[1];
+            if (ho[1] > 0) {
+                CUDA_TRY(h, cudaEventRecord(h->evb[6], st));
+                const int rc2 = run_cta(3, cap, ovf_b, ho[1], dcnt + 15, 48 * 1024);
+                if (rc2 != MSPAI_OK)
+                    return rc2;
+                CUDA_TRY(h, cudaEventRecord(h->evb[7], st));
+                timed[3] = true;
+            }
         }
         else {
-            // shared memory for the folded matrix: the bucket's worst case when
-            // it is small, else a large area (one CTA per SM) that holds W when
-            // it fits and stages the QR panels when it does not
-            size_t wsm = std::min<size_t>(mspai::w_bytes(cap, elem), h->smem_budget);
-            if (!prm->batched)
-                wsm = 0;  // the plain path keeps W in global memory, unblocked
-            const size_t need = mspai::cta_scratch_needed(elem, cap, count, wsm);
-            CUDA_TRY(h, h->scratch.ensure(need));
-            if (adaptive)  // the candidate bit vectors of the slots start cleared
-                CUDA_TRY(h, cudaMemsetAsync(h->scratch.p, 0, need, st));
-            h->launches++;
-            CUDA_TRY(h, mspai::launch_cta_solve(elem, wsm, prm->batched != 0, pb, cap, out, list,
-                                                count, counter,
-                                                h->scratch.as<char>(), h->scratch.bytes, st,
-                                                &grid));
+            CUDA_TRY(h, cudaEventRecord(h->evb[2 * b], st));
+            const int rc2 = run_cta(b, cap, list, count, counter, h->smem_budget);
+            if (rc2 != MSPAI_OK)
+                return rc2;
+            CUDA_TRY(h, cudaEventRecord(h->evb[2 * b + 1], st));
+            timed[b] = true;
+            h->stats.bucket_columns[b] = count;
         }
-        CUDA_TRY(h, cudaEventRecord(h->evb[2 * b + 1], st));
     }
 
     if (reuse) {
@@ -672,11 +759,11 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     float ms = 0.f;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     h->stats.setup_ms = ms;
-    for (int b = 0; b < kBuckets; b++) {
-        if (hc[b] > 0) {
+    for (int k = 0; k < kKernels; k++) {
+        if (timed[k]) {
             float kms = 0.f;
-            cudaEventElapsedTime(&kms, h->evb[2 * b], h->evb[2 * b + 1]);
-            h->stats.kernel_ms[b] = kms;
+            cudaEventElapsedTime(&kms, h->evb[2 * k], h->evb[2 * k + 1]);
+            h->stats.kernel_ms[k] = kms;
         }
     }
     h->stats.reused_columns = 0;
@@ -844,17 +931,29 @@ int mspai_get_stats(mspai_handle* h, mspai_stats* s)
     }
     double fl = 0.0, fld = 0.0, by = 0.0;
     int64_t solves = 0, sing = 0, capc = 0;
-    // algorithmic flops per bucket kernel (columns listed per bucket)
+    // algorithmic flops per solver launch: the columns of its work list that
+    // it solved (a fixed-pattern launch passes the columns it could not hold
+    // on to the next list)
     for (int b = 0; b < 4; b++)
         h->stats.bucket_flops[b] = 0.0;
     if (h->nprob > 0 && h->lists.p) {
-        std::vector<int32_t> lists(static_cast<size_t>(kBuckets) * h->nprob);
+        std::vector<int32_t> lists(static_cast<size_t>(kLists) * h->nprob);
         CUDA_TRY(h, cudaMemcpy(lists.data(), h->lists.p, sizeof(int32_t) * lists.size(),
                                cudaMemcpyDeviceToHost));
-        for (int b = 0; b < kBuckets; b++)
-            for (int64_t t = 0; t < h->stats.bucket_columns[b]; t++)
-                h->stats.bucket_flops[b] +=
-                    work[3 * static_cast<size_t>(lists[b * static_cast<size_t>(h->nprob) + t])];
+        double sums[kLists] = {0.0, 0.0, 0.0, 0.0};
+        for (int b = 0; b < kLists; b++)
+            for (int64_t t = 0; t < h->list_len[b]; t++)
+                sums[b] += work[3 * static_cast<size_t>(lists[b * static_cast<size_t>(h->nprob) + t])];
+        if (h->used_fixed) {
+            h->stats.bucket_flops[0] = sums[0];
+            h->stats.bucket_flops[1] = sums[1] - sums[2];
+            h->stats.bucket_flops[2] = sums[2] - sums[3];
+            h->stats.bucket_flops[3] = sums[3];
+        }
+        else {
+            for (int b = 0; b < kBuckets; b++)
+                h->stats.bucket_flops[b] = sums[b];
+        }
     }
     for (int c = 0; c < h->n; c++) {
         fl += work[3 * c];

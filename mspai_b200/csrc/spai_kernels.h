@@ -69,6 +69,19 @@ cudaError_t launch_cta_solve(int elem_bytes, size_t smem_w_bytes, bool blocked,
                              const Problem& pb, const Caps& cap, const Output& out,
                              const int32_t* list, int count, int32_t* counter, char* scratch,
                              size_t scratch_bytes, cudaStream_t st, int* grid_out);
+// Fixed-pattern scalar solver (fixed_kernels.cu): columns list[0 .. count)
+// (count from count_dev when not null, else count_host); columns that do not
+// fit the arena of arena_bytes go to ovf_list / *ovf_count.  rglob: per-CTA
+// areas of rglob_elems elements for R when it does not fit the arena (null:
+// such columns overflow).
+int fixed_ctas_per_sm(int arena_bytes);
+int fixed_max_grid(int arena_bytes);
+int64_t fixed_r_elems(int nmax);
+cudaError_t launch_fixed_solve(int elem_bytes, int arena_bytes, const Problem& pb,
+                               const Output& out, const int32_t* list, const int32_t* count_dev,
+                               int count_host, int32_t* counter, int32_t* ovf_list,
+                               int32_t* ovf_count, void* rglob, int64_t rglob_elems, int max_ctas,
+                               cudaStream_t st, int* grid_out);
 cudaError_t launch_scan_lengths(const int32_t* len, int n, int64_t* ptr, int64_t* tmp,
                                 cudaStream_t st);
 cudaError_t launch_capacity_len(const int64_t* pptr, int n, int bs, int grow, int32_t* len,

@@ -35,12 +35,12 @@ def load():
         lib.oracle_spai_scalar.argtypes = [
             ctypes.c_int, ctypes.c_int, P, P, P, P, P, P, P, P, P, P, P, P,
             ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
-            ctypes.c_int, ctypes.c_int, P, P, P, P, P, P]
+            ctypes.c_int, ctypes.c_int, P, P, P, P, P, P, P]
         lib.oracle_spai_block.restype = ctypes.c_int
         lib.oracle_spai_block.argtypes = [
             ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, P, P, P, P, P, P, P,
             ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
-            ctypes.c_int, ctypes.c_int, P, P, P, P, P, P]
+            ctypes.c_int, ctypes.c_int, P, P, P, P, P, P, P]
         _lib = lib
     return _lib
 
@@ -78,7 +78,9 @@ class OracleResult:
 
 def spai_scalar(C: sp.csc_matrix, P: sp.csc_matrix, *, B: Optional[sp.csc_matrix] = None,
                 UP: Optional[sp.csc_matrix] = None, ep: float = 0.4, mn: int = 5, ns: int = 5,
-                um: int = 1, cols: Optional[tuple] = None) -> OracleResult:
+                um: int = 1, cols: Optional[tuple] = None,
+                col_list: Optional[np.ndarray] = None) -> OracleResult:
+    """Columns [cols[0], cols[1]) (all when None), or the columns in col_list."""
     lib = load()
     C = sp.csc_matrix(C, dtype=np.float64)
     C.sort_indices()
@@ -107,7 +109,12 @@ def spai_scalar(C: sp.csc_matrix, P: sp.csc_matrix, *, B: Optional[sp.csc_matrix
         UP.sort_indices()
         upptr = np.ascontiguousarray(UP.indptr, dtype=np.int64)
         upidx = np.ascontiguousarray(UP.indices, dtype=np.int32)
-    lo, hi = (0, n) if cols is None else cols
+    lst = None
+    if col_list is not None:
+        lst = np.ascontiguousarray(col_list, dtype=np.int32)
+        lo, hi = 0, len(lst)
+    else:
+        lo, hi = (0, n) if cols is None else cols
     stride = int(np.diff(pptr).max()) + mn * ns + 1
     out_len = np.zeros(n, dtype=np.int32)
     out_idx = np.zeros(n * stride, dtype=np.int32)
@@ -120,7 +127,7 @@ def spai_scalar(C: sp.csc_matrix, P: sp.csc_matrix, *, B: Optional[sp.csc_matrix
                                 _ptr(pidx), _ptr(upptr), _ptr(upidx), float(ep), int(mn),
                                 int(ns), int(um), int(lo), int(hi), stride, _ptr(out_len),
                                 _ptr(out_idx), _ptr(out_val), _ptr(out_res), _ptr(out_steps),
-                                _ptr(out_info))
+                                _ptr(out_info), _ptr(lst))
     if rc != 0:
         raise RuntimeError(f"oracle failed ({rc})")
     lens = out_len.astype(np.int64)
@@ -133,8 +140,10 @@ def spai_scalar(C: sp.csc_matrix, P: sp.csc_matrix, *, B: Optional[sp.csc_matrix
 
 def spai_block(C: sp.csc_matrix, Pb: sp.csc_matrix, bs: int, *,
                B: Optional[sp.csc_matrix] = None, ep: float = 0.4, mn: int = 5, ns: int = 5,
-               um: int = 1, blocks: Optional[tuple] = None) -> OracleResult:
-    """Block SPAI with constant block size bs; Pb is the (n/bs x n/bs) block pattern."""
+               um: int = 1, blocks: Optional[tuple] = None,
+               block_list: Optional[np.ndarray] = None) -> OracleResult:
+    """Block SPAI with constant block size bs; Pb is the (n/bs x n/bs) block pattern.
+    Block columns [blocks[0], blocks[1]) (all when None), or those in block_list."""
     lib = load()
     C = sp.csc_matrix(C, dtype=np.float64)
     C.sort_indices()
@@ -158,7 +167,12 @@ def spai_block(C: sp.csc_matrix, Pb: sp.csc_matrix, bs: int, *,
         bidx = np.ascontiguousarray(B.indices, dtype=np.int32)
         bval = np.ascontiguousarray(B.data, dtype=np.float64)
     nb = n // bs
-    lo, hi = (0, nb) if blocks is None else blocks
+    lst = None
+    if block_list is not None:
+        lst = np.ascontiguousarray(block_list, dtype=np.int32)
+        lo, hi = 0, len(lst)
+    else:
+        lo, hi = (0, nb) if blocks is None else blocks
     stride = bs * (int(np.diff(pptr).max()) + mn * ns) + 1
     out_len = np.zeros(n, dtype=np.int32)
     out_idx = np.zeros(n * stride, dtype=np.int32)
@@ -170,7 +184,7 @@ def spai_block(C: sp.csc_matrix, Pb: sp.csc_matrix, bs: int, *,
                                _ptr(rcol), _ptr(bptr), _ptr(bidx), _ptr(bval), _ptr(pptr),
                                _ptr(pidx), float(ep), int(mn), int(ns), int(um), int(lo),
                                int(hi), stride, _ptr(out_len), _ptr(out_idx), _ptr(out_val),
-                               _ptr(out_res), _ptr(out_steps), _ptr(out_info))
+                               _ptr(out_res), _ptr(out_steps), _ptr(out_info), _ptr(lst))
     if rc != 0:
         raise RuntimeError(f"oracle failed ({rc})")
     lens = out_len.astype(np.int64)

@@ -31,7 +31,12 @@
  *
  * Extra driver options (not in the reference):
  *   -cols a:b   run SPAI_Column for columns [a, b) only (timed subset)
+ *   -colfile f  run SPAI_Column for the (block) columns listed in f, one index
+ *               per line (a stratified sample of a large problem)
  *   -time f     write {"setup_s":…, "columns":…} as JSON to file f
+ * With a subset, only the computed columns are written (scalar columns; a
+ * block column as its bs scalar columns, through the reference's
+ * Matrix::Scalar_Matrix).
  */
 #include "Matrix.h"
 #include "Pattern.h"
@@ -46,6 +51,7 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 namespace {
 
@@ -64,6 +70,7 @@ struct Options {
     const char* be = nullptr;
     const char* out = "precond.mtx";
     long col_lo = -1, col_hi = -1;
+    const char* col_file = nullptr;
     const char* time_file = nullptr;
 };
 
@@ -73,7 +80,7 @@ void usage()
                  "usage: ref_driver <A.mtx> <pattern.mtx|-1|-2> <B.mtx|-1> [-ep x] [-mn k] "
                  "[-ns k] [-hs k] [-cs k] [-qr k] [-fg x] [-um 0|1] [-ch 0|1] [-Ce f] [-Be f] "
                  "[-rho x] [-schur 0|1] [-up f|1|2] [-pk k] [-pm 0|1] [-bs k] [-vb k] "
-                 "[-out f] [-cols a:b] [-time f]\n");
+                 "[-out f] [-cols a:b] [-colfile f] [-time f]\n");
     std::exit(2);
 }
 
@@ -126,6 +133,7 @@ Options parse(int argc, char** argv)
             else if (!std::strcmp(v, "2")) o.up = 2;
             else { o.up = 0; o.up_file = v; }
         }
+        else if (k == "-colfile") o.col_file = v;
         else if (k == "-cols") {
             if (std::sscanf(v, "%ld:%ld", &o.col_lo, &o.col_hi) != 2)
                 usage();
@@ -258,11 +266,23 @@ int main(int argc, char** argv)
         if (hash_param > 0)
             M->ht_M = new Hash_Table<double>(hash_param);
 
-        long lo = 0, hi = A_sys->n;
-        const bool subset = o.col_lo >= 0;
-        if (subset) {
-            lo = o.col_lo < 0 ? 0 : o.col_lo;
-            hi = o.col_hi > A_sys->n ? A_sys->n : o.col_hi;
+        // the columns to compute: all, a range, or a list
+        std::vector<long> cols;
+        const bool subset = o.col_lo >= 0 || o.col_file != nullptr;
+        if (o.col_file) {
+            FILE* cf = std::fopen(o.col_file, "r");
+            if (!cf)
+                throw std::runtime_error("cannot read the column file");
+            long c = 0;
+            while (std::fscanf(cf, "%ld", &c) == 1)
+                if (c >= 0 && c < A_sys->n)
+                    cols.push_back(c);
+            std::fclose(cf);
+        }
+        else if (o.col_lo >= 0) {
+            const long hi = o.col_hi > A_sys->n ? A_sys->n : o.col_hi;
+            for (long c = o.col_lo; c < hi; c++)
+                cols.push_back(c);
         }
 
         auto t0 = std::chrono::steady_clock::now();
@@ -272,7 +292,7 @@ int main(int argc, char** argv)
         }
         else {
             // Same per-run set-up as SPAI_Algorithm (src/Spai.imp:67-120), then
-            // the reference's column routine on [lo, hi).
+            // the reference's column routine on the listed columns.
             if (o.ns > 0)
                 M->Precomputation_Column_Square_Inverses(A_sys);
             int bitvec_size = A_sys->m <= A_sys->n ? A_sys->n : A_sys->m;
@@ -281,7 +301,7 @@ int main(int argc, char** argv)
             unsigned int* bitvec = M->bitvec;
             unsigned int* reset_vec = M->reset_vec;
             auto fn = Column_Access::fn();
-            for (long col = lo; col < hi; col++)
+            for (long col : cols)
                 (alg->*fn)(A_sys, M, B, P, UP, nullptr, static_cast<int>(col), o.ep, o.mn, o.ns,
                            M->ht_M, o.um, o.pk, o.pm, bitvec, reset_vec);
         }
@@ -291,7 +311,8 @@ int main(int argc, char** argv)
         if (o.time_file) {
             FILE* f = std::fopen(o.time_file, "w");
             if (f) {
-                std::fprintf(f, "{\"setup_s\": %.9f, \"columns\": %ld}\n", secs, hi - lo);
+                std::fprintf(f, "{\"setup_s\": %.9f, \"columns\": %ld}\n", secs,
+                             subset ? static_cast<long>(cols.size()) : static_cast<long>(A_sys->n));
                 std::fclose(f);
             }
         }
@@ -305,21 +326,28 @@ int main(int argc, char** argv)
             }
         }
         else {
-            // Columns [lo, hi) only, in the reference's output format, so the
-            // subset can be compared column by column.
+            // The computed columns only, in the reference's output format, so
+            // the subset can be compared column by column (block columns as
+            // their scalar columns)
+            Matrix<double>* S = (o.bs != 1) ? M->Scalar_Matrix(0) : M;
+            const int bsz = (o.bs != 1) ? o.bs : 1;
             FILE* f = std::fopen(o.out, "w");
             if (!f)
                 throw std::runtime_error("cannot write output");
             long nnz = 0;
-            for (long c = lo; c < hi; c++)
-                nnz += M->c_lines->len_cols[c];
+            for (long c : cols)
+                for (int q = 0; q < bsz; q++)
+                    nnz += S->c_lines->len_cols[c * bsz + q];
             std::fprintf(f, "%%%%MatrixMarket matrix coordinate real general\n%d %d %ld\n",
-                         M->m, M->n, nnz);
-            for (long c = lo; c < hi; c++)
-                for (int i = 0; i < M->c_lines->len_cols[c]; i++) {
-                    double v = M->c_lines->A[c][i];
-                    std::fprintf(f, "%d %ld%s%.13e\n", M->c_lines->col_idcs[c][i] + 1, c + 1,
-                                 v < 0.0 ? " " : "  ", v);
+                         S->m, S->n, nnz);
+            for (long c : cols)
+                for (int q = 0; q < bsz; q++) {
+                    const long sc = c * bsz + q;
+                    for (int i = 0; i < S->c_lines->len_cols[sc]; i++) {
+                        double v = S->c_lines->A[sc][i];
+                        std::fprintf(f, "%d %ld%s%.13e\n", S->c_lines->col_idcs[sc][i] + 1,
+                                     sc + 1, v < 0.0 ? " " : "  ", v);
+                    }
                 }
             std::fclose(f);
         }

@@ -154,7 +154,8 @@ int ls_solve(std::vector<double> A, int m, int n, int nrhs, double* x, int ldx)
 extern "C" {
 
 /*
- * Scalar SPAI / MSPAI setup for columns [col_lo, col_hi).
+ * Scalar SPAI / MSPAI setup for columns [col_lo, col_hi), or, when col_list
+ * is not null, for the columns col_list[col_lo .. col_hi).
  *
  * C      : nrows x n CSC (rows >= n are probing rows), sorted rows.
  * Crow   : CSR row structure of C's first n rows (column indices per row,
@@ -172,7 +173,8 @@ int oracle_spai_scalar(int nrows, int n, const int64_t* cptr, const int32_t* cid
                        const int64_t* pptr, const int32_t* pidx, const int64_t* upptr,
                        const int32_t* upidx, double ep, int mn, int ns, int um, int col_lo,
                        int col_hi, int out_stride, int32_t* out_len, int32_t* out_idx,
-                       double* out_val, double* out_res, int32_t* out_steps, int32_t* out_info)
+                       double* out_val, double* out_res, int32_t* out_steps, int32_t* out_info,
+                       const int32_t* col_list)
 {
     Csc C{nrows, n, cptr, cidx, cval};
     Csc Bm{nrows, n, bptr, bidx, bval};
@@ -182,7 +184,8 @@ int oracle_spai_scalar(int nrows, int n, const int64_t* cptr, const int32_t* cid
     std::vector<double> Ahat, b, bk, r;
     std::vector<RhoIdx> rhos;
 
-    for (int col = col_lo; col < col_hi; col++) {
+    for (int it = col_lo; it < col_hi; it++) {
+        const int col = col_list ? col_list[it] : it;
         // Com_Server::Get_P_Col (src/Com_Server.imp:446-470)
         J.assign(pidx + pptr[col], pidx + pptr[col + 1]);
         double res = 1.0e50;
@@ -326,7 +329,7 @@ int oracle_spai_block(int nrows, int n_s, int bs, const int64_t* cptr, const int
                       const int64_t* pbptr, const int32_t* pbidx, double ep, int mn, int ns,
                       int um, int kb_lo, int kb_hi, int out_stride, int32_t* out_len,
                       int32_t* out_idx, double* out_val, double* out_res, int32_t* out_steps,
-                      int32_t* out_info)
+                      int32_t* out_info, const int32_t* blk_list)
 {
     const int nb = n_s / bs;
     if (nb * bs != n_s)
@@ -339,7 +342,8 @@ int oracle_spai_block(int nrows, int n_s, int bs, const int64_t* cptr, const int
     std::vector<int> J, I, L, U, Jt, rowoff;
     std::vector<double> Ahat, E, X, R;
     std::vector<RhoIdx> rhos;
-    for (int kb = kb_lo; kb < kb_hi; kb++) {
+    for (int it = kb_lo; it < kb_hi; it++) {
+        const int kb = blk_list ? blk_list[it] : it;  // block columns [lo, hi) or a list
         J.assign(pbidx + pbptr[kb], pbidx + pbptr[kb + 1]);
         double res = 1.0e50;
         int steps = 0, info = 0;

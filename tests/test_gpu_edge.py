@@ -96,8 +96,7 @@ def test_warp_bucket_limits(h):
         h.setup(A, P, options=mb.Options(ns=0, prec=prec))
         M = h.result()
         st = h.stats()
-        assert st["bucket_columns"][0] > 0 and st["bucket_columns"][0] + st["bucket_columns"][1] \
-            + st["bucket_columns"][2] == n
+        assert st["bucket_columns"][0] > 0 and sum(st["bucket_columns"]) == n
         o = O.spai_scalar(A, P, ns=0)
         assert same_pattern(M, o.M)
         assert max_rel_diff(M, o.M) < (1e-10 if prec == "fp64" else 1e-8)

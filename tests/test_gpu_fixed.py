@@ -1,0 +1,162 @@
+"""The fixed-pattern column solver (fixed_solve.cuh) against the oracle and the
+reference's own output.
+
+Fixed scalar patterns whose columns are larger than the warp bucket's (more
+than 64 entries of C(:, J_k) or |J_k| > 16) go through it: the patterns here
+are pattern(A^2), so every interior column of the stencils qualifies.
+Tolerances: identical patterns; every value within 1e-10 (FP64) / 1e-8
+(mixed) of its own magnitude, entries below 1e-3 of their column's largest
+against that floor (helpers.max_rel_diff); residual norms within 1e-9.
+The overflow chain (first launch -> large-arena launch -> general solver) is
+exercised by shrinking the arenas through the library's environment knobs."""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import mspai_b200 as mb
+from conftest import load_golden
+from helpers import column_residuals, max_rel_diff, same_pattern
+from mspai_b200 import workloads as W
+from oracle import pyoracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-10, "mixed": 1e-8}
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+@pytest.fixture(scope="module")
+def h():
+    handle = mb.Handle(0)
+    yield handle
+    handle.close()
+
+
+def square_pattern(A):
+    return W.square_pattern_dropped(A, drop=0.0)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("nx", [12, 20])
+def test_poisson_pattern_a2_against_oracle(h, nx, prec):
+    w = W.poisson2d(nx)
+    P = square_pattern(w.A)
+    h.setup(w.A, P, options=mb.Options(ns=0, prec=prec))
+    M = h.result()
+    st = h.stats()
+    assert st["bucket_columns"][1] + st["bucket_columns"][2] + st["bucket_columns"][3] > 0
+    o = O.spai_scalar(w.A, P, ns=0)
+    assert same_pattern(M, o.M)
+    assert max_rel_diff(M, o.M) < TOL[prec]
+    res, steps, status = h.column_info()
+    assert np.all(status == 0) and np.all(steps == 1)
+    assert np.allclose(res, o.res, rtol=1e-9, atol=1e-14)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("kinds,rho", [(("ones",), 10.0), (("ones", "alt"), 100.0)])
+def test_probing_target_pattern_a2(h, prec, kinds, rho):
+    """C = [A; rho Ce] with B = [I; rho Be]: the probing rows are shared rows of
+    every column, B's probing entries are targets of shared rows."""
+    w = W.aniso2d_probing(14, kinds=kinds, rho=rho)
+    C, B = mb.assemble_probing(w.A, w.Ce, w.Be, rho)
+    P = square_pattern(w.A)
+    h.setup(C, P, B=B, options=mb.Options(ns=0, prec=prec, probing=1, rho=rho))
+    M = h.result()
+    o = O.spai_scalar(C, P, B=B, ns=0)
+    assert same_pattern(M, o.M)
+    assert max_rel_diff(M, o.M) < TOL[prec]
+    res, _, status = h.column_info()
+    assert np.all(status == 0)
+    assert np.allclose(res, o.res, rtol=1e-9, atol=1e-14)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_ragged_reference_output(h, prec):
+    w = W.ragged(3000)
+    h.setup(w.A, w.P, options=mb.Options(ns=0, prec=prec))
+    M = h.result()
+    ref = load_golden("ragged_3000")
+    assert same_pattern(M, ref)
+    assert max_rel_diff(M, ref) < max(TOL[prec], 5e-12)
+    res, _, status = h.column_info()
+    assert np.all(status == 0)
+    assert np.allclose(res, column_residuals(w.A, M), rtol=1e-9, atol=1e-13)
+
+
+def test_singular_and_empty_target_columns(h):
+    """k outside I_k gives b = 0 and m_k = 0; a pattern whose columns repeat the
+    same column of A makes R singular (status 1, dtrtrs leaves Q^T b)."""
+    w = W.poisson2d(10)
+    n = w.n
+    P2 = square_pattern(w.A).tolil()
+    far = (np.arange(n) + 37) % n
+    for k in range(0, n, 7):  # these columns only see rows far from k
+        P2[:, k] = 0
+        P2[far[k], k] = 1
+    P2 = sp.csc_matrix(P2)
+    h.setup(w.A, P2, options=mb.Options(ns=0, prec="fp64"))
+    M = h.result()
+    o = O.spai_scalar(w.A, P2, ns=0)
+    assert same_pattern(M, o.M)
+    assert max_rel_diff(M, o.M) < 1e-10
+
+
+CHAIN = r"""
+import os, sys, json
+sys.path.insert(0, {root!r})
+import numpy as np
+import mspai_b200 as mb
+from mspai_b200 import workloads as W
+w = W.ragged(4000)
+h = mb.Handle(0)
+out = {{}}
+for prec in ("fp64", "mixed"):
+    h.setup(w.A, w.P, options=mb.Options(ns=0, prec=prec))
+    M = h.result()
+    res, steps, status = h.column_info()
+    st = h.stats()
+    np.save(os.path.join({tmp!r}, prec + "_vals.npy"), M.data)
+    np.save(os.path.join({tmp!r}, prec + "_res.npy"), res)
+    out[prec] = {{"buckets": [int(v) for v in st["bucket_columns"]],
+                 "status_ok": bool(np.all(status == 0))}}
+print(json.dumps(out))
+"""
+
+
+@pytest.mark.parametrize("arena,large", [("16", "216"), ("8", "24"), ("4", "4")])
+def test_overflow_chain_gives_identical_columns(tmp_path, arena, large):
+    """Shrunken arenas push columns from the first launch to the large-arena
+    launch and on to the general solver; each path solves the same problems
+    (values within the tolerances of the default run, same residuals)."""
+    def run(env_extra, tag):
+        d = tmp_path / tag
+        d.mkdir()
+        env = dict(os.environ, **env_extra)
+        code = CHAIN.format(root=os.path.dirname(HERE), tmp=str(d))
+        r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        import json
+        return json.loads(r.stdout.strip().splitlines()[-1]), d
+    base, dbase = run({}, "base")
+    small, dsmall = run({"MSPAI_FIXED_ARENA_KB": arena, "MSPAI_FIXED_ARENA_LARGE_KB": large},
+                        "small")
+    for prec in ("fp64", "mixed"):
+        assert base[prec]["status_ok"] and small[prec]["status_ok"]
+        b1 = small[prec]["buckets"]
+        if arena == "4":
+            assert b1[1] == 0 and b1[2] == 0 and b1[3] > 0  # everything to the general solver
+        else:
+            assert b1[2] + b1[3] > 0  # the chain was used
+        va = np.load(dbase / f"{prec}_vals.npy")
+        vb = np.load(dsmall / f"{prec}_vals.npy")
+        scale = np.maximum(np.abs(va), 1e-3 * np.max(np.abs(va)))
+        assert np.max(np.abs(va - vb) / scale) < TOL[prec]
+        ra = np.load(dbase / f"{prec}_res.npy")
+        rb = np.load(dsmall / f"{prec}_res.npy")
+        assert np.allclose(ra, rb, rtol=1e-9, atol=1e-14)
