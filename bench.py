@@ -115,69 +115,86 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ reference arm helpers
-def write_subproblem(w, cols, directory):
-    """Matrix Market files of the sub-problem that columns [0, cols) see.
+REF_COLS_PER_PROC = 800   # about 5 s of the reference's column loop per process
+REF_MAX_PROCS = 64        # each process holds the sub-problem (~0.5 GB)
 
-    Columns of A outside the union of J_k (k < cols) are replaced by unit
+
+def sample_columns(P, total, seed=0x5A11):
+    """`total` columns stratified by |J_k|: an equal share from each of 8
+    equal-count strata of the pattern sizes (seeded), in random order."""
+    sizes = np.diff(P.indptr)
+    order = np.argsort(sizes, kind="stable")
+    rng = np.random.default_rng(seed)
+    parts = np.array_split(order, 8)
+    share = [total // 8 + (1 if i < total % 8 else 0) for i in range(8)]
+    cols = np.concatenate([rng.choice(p, size=min(s_, len(p)), replace=False)
+                           for p, s_ in zip(parts, share)])
+    rng.shuffle(cols)
+    return cols
+
+
+def write_subproblem(w, cols, directory):
+    """Matrix Market files of the sub-problem that the listed columns see.
+
+    Columns of A outside the union of J_k (k listed) are replaced by unit
     columns (never read by those columns' least-squares problems: ns = 0);
-    the pattern keeps J_k for k < cols and is diagonal elsewhere.  The
-    reference therefore computes exactly the columns [0, cols) of the full
+    the pattern keeps J_k for the listed k and is diagonal elsewhere.  The
+    reference therefore computes exactly the listed columns of the full
     setup."""
     import scipy.sparse as sp
     from mspai_b200 import workloads as W
     A = sp.csc_matrix(w.A)
     P = sp.csc_matrix(w.P)
     n = A.shape[1]
-    used = np.unique(P.indices[: P.indptr[cols]])
     keep = np.zeros(n, dtype=bool)
-    keep[used] = True
+    for k in cols:
+        keep[P.indices[P.indptr[k]:P.indptr[k + 1]]] = True
     lens = np.diff(A.indptr)
     colmask = np.repeat(keep, lens)
-    rows_kept = A.indices[colmask]
-    cols_kept = np.repeat(np.arange(n), lens)[colmask]
-    vals_kept = A.data[colmask]
     other = np.nonzero(~keep)[0]
-    Asub = sp.csc_matrix((np.concatenate([vals_kept, np.ones(len(other))]),
-                          (np.concatenate([rows_kept, other]), np.concatenate([cols_kept, other]))),
+    Asub = sp.csc_matrix((np.concatenate([A.data[colmask], np.ones(len(other))]),
+                          (np.concatenate([A.indices[colmask], other]),
+                           np.concatenate([np.repeat(np.arange(n), lens)[colmask], other]))),
                          shape=(n, n))
-    prow = np.concatenate([P.indices[: P.indptr[cols]], np.arange(cols, n)])
-    pcol = np.concatenate([np.repeat(np.arange(cols), np.diff(P.indptr)[:cols]), np.arange(cols, n)])
+    sel = np.zeros(n, dtype=bool)
+    sel[cols] = True
+    plen = np.diff(P.indptr)
+    pmask = np.repeat(sel, plen)
+    prow = np.concatenate([P.indices[pmask], np.nonzero(~sel)[0]])
+    pcol = np.concatenate([np.repeat(np.arange(n), plen)[pmask], np.nonzero(~sel)[0]])
     Psub = sp.csc_matrix((np.ones(len(prow)), (prow, pcol)), shape=(n, n))
     W.write_mm(os.path.join(directory, "A.mtx"), Asub)
     W.write_mm(os.path.join(directory, "P.mtx"), Psub, pattern=True)
 
 
-def run_reference_sample(directory, lo, hi, tag):
-    """Times the reference's SPAI_Column loop on columns [lo, hi) (1 thread)."""
+def reference_step_times(directory, chunks, reps):
+    """Runs the reference's SPAI_Column loop, one process per chunk of columns
+    (OPENBLAS_NUM_THREADS=1), `reps` passes after one read of the inputs.
+    Returns the per-pass wall time of the slowest process (s), per pass."""
     env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS="1")
-    tfile = os.path.join(directory, f"t_{tag}.json")
-    return subprocess.Popen([REF_DRIVER, "A.mtx", "P.mtx", "-1", "-ns", "0", "-cols",
-                             f"{lo}:{hi}", "-time", tfile, "-out", f"M_{tag}.mtx"],
-                            cwd=directory, env=env, stdout=subprocess.DEVNULL,
-                            stderr=subprocess.DEVNULL), tfile
-
-
-def cpu_reference_rate(w, cols_per_proc, procs, directory, write=True):
-    """columns/s of the reference on `procs` host cores (one process each)."""
-    if write:
-        write_subproblem(w, cols_per_proc * procs, directory)
     jobs = []
-    for p in range(procs):
-        jobs.append(run_reference_sample(directory, p * cols_per_proc, (p + 1) * cols_per_proc, p))
-    secs = []
-    for proc, tfile in jobs:
+    for p, chunk in enumerate(chunks):
+        cf = os.path.join(directory, f"cols_{p}.txt")
+        np.savetxt(cf, np.asarray(chunk, dtype=np.int64), fmt="%d")
+        tf = os.path.join(directory, f"t_{p}.json")
+        jobs.append((subprocess.Popen(
+            [REF_DRIVER, "A.mtx", "P.mtx", "-1", "-ns", "0", "-colfile", cf, "-repeat", str(reps),
+             "-time", tf, "-out", f"M_{p}.mtx"], cwd=directory, env=env,
+            stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL), tf))
+    per_proc = []
+    for proc, tf in jobs:
         if proc.wait() != 0:
             raise RuntimeError("reference driver failed")
-        secs.append(json.load(open(tfile))["setup_s"])
-    return cols_per_proc * procs / max(secs), max(secs)
+        per_proc.append(json.load(open(tf))["rep_s"])
+    return [max(r[i] for r in per_proc) for i in range(reps)]
 
 
 def oracle_port_rate(w, cols):
     from oracle import pyoracle
     t0 = time.perf_counter()
-    pyoracle.spai_scalar(w.A, w.P, ns=0, cols=(0, cols))
+    pyoracle.spai_scalar(w.A, w.P, ns=0, col_list=cols)
     dt = time.perf_counter() - t0
-    return cols / dt, dt
+    return len(cols) / dt, dt
 
 
 # ------------------------------------------------------------------ main paths
@@ -238,28 +255,31 @@ def bench_reference(args):
         return 0
     from mspai_b200 import workloads as W
     w = W.ragged(args.n, seed=BASE_SEED)
-    procs = max(1, os.cpu_count() or 1)
-    per = 4
+    procs = max(1, min(os.cpu_count() or 1, REF_MAX_PROCS))
+    cols = sample_columns(w.P, REF_COLS_PER_PROC * procs)
+    chunks = np.array_split(cols, procs)
+    warm = max(args.warmup, 1)
     with tempfile.TemporaryDirectory() as d:
-        write_subproblem(w, per * procs, d)
-        for _ in range(args.warmup):
-            cpu_reference_rate(w, per, procs, d, write=False)
-        rates, secs = [], []
-        for _ in range(args.steps):
-            r, s = cpu_reference_rate(w, per, procs, d, write=False)
-            rates.append(r)
-            secs.append(s)
-    value = float(np.median(rates))
-    sample = (f"columns [0, {per * procs}) of the {args.n}-column workload, {per} per process, "
-              f"{procs} processes (OPENBLAS_NUM_THREADS=1), reference SPAI_Column loop")
+        write_subproblem(w, cols, d)
+        steps = reference_step_times(d, chunks, warm + args.steps)[warm:]
+        # the same work on one core: the first process's share alone
+        one = reference_step_times(d, chunks[:1], 2)[-1]
+    secs = float(np.median(steps))
+    value = len(cols) / secs
+    rate1 = len(chunks[0]) / one
+    sample = (f"{len(cols)} columns of the {args.n}-column workload stratified by |J_k| "
+              f"(8 equal-count strata, seeded), {len(chunks[0])} per process, {procs} processes "
+              f"(OPENBLAS_NUM_THREADS=1), reference SPAI_Column loop; step = one pass, the "
+              f"slowest process's time")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": float(np.median(secs)) * 1e3, "higher_is_better": True,
+        "ms_per_step": secs * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(args.n),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
-                         "sample": sample},
+                         "sample": sample, "one_core_value": rate1,
+                         "cores_speedup": value / rate1},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
     return 0
@@ -359,6 +379,27 @@ def bench_ours(args):
                              "frob_AM_minus_I_fp64": frob_plain,
                              "frob_rel_diff": abs(frob_mixed - frob_plain) / frob_plain}
 
+    # the same batched kernels in FP64 (no refinement): isolates the gain of
+    # the mixed precision from that of the batched design
+    if not args.no_plain:
+        bf = mb.Options(ns=0, prec="fp64", batched=True)
+        h.setup(dA, dP, options=bf)
+        torch.cuda.synchronize()
+        b0 = torch.cuda.Event(enable_timing=True)
+        b1 = torch.cuda.Event(enable_timing=True)
+        b0.record(stream)
+        h.setup(dA, dP, options=bf)
+        b1.record(stream)
+        torch.cuda.synchronize()
+        bms = max_over_ranks(b0.elapsed_time(b1), world)
+        res_b, _, _ = h.column_info()
+        frob_b = float(np.sqrt(np.sum(res_b ** 2)))
+        out["batched_fp64"] = {"value": world * n / (bms * 1e-3), "unit": UNIT,
+                               "ms_per_step": bms,
+                               "mixed_over_batched_fp64": bms / ms,
+                               "frob_AM_minus_I": frob_b,
+                               "frob_rel_diff_mixed": abs(frob_mixed - frob_b) / frob_b}
+
     # end to end through the public API from pinned host memory
     if not args.no_e2e:
         hA = mb.DeviceCSC.from_scipy(w.A, device="cpu", pin=True)
@@ -386,23 +427,25 @@ def bench_ours(args):
                       "d2h_bytes_per_step": oc.numel() * 8 + oi.numel() * 4 + ov.numel() * 8,
                       "ms_per_step": ems}
 
-    # CPU baseline: the reference's column loop on a bounded sample, 1 core
+    # CPU baseline: the reference's column loop on a bounded sample (one
+    # process's share of the reference arm's stratified sample), 1 core
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
+            cols = sample_columns(w.P, REF_COLS_PER_PROC)
             if os.path.exists(REF_DRIVER):
-                cols = 48
                 with tempfile.TemporaryDirectory() as d:
-                    rate, secs = cpu_reference_rate(w, cols, 1, d)
+                    write_subproblem(w, cols, d)
+                    secs = reference_step_times(d, [cols], 2)[-1]
                 out["cpu_baseline"] = {
-                    "value": rate, "unit": UNIT, "cores": 1, "kind": "reference",
-                    "sample": f"columns [0, {cols}) of this workload, reference SPAI_Column "
-                              f"loop, 1 thread ({secs:.1f} s)"}
+                    "value": len(cols) / secs, "unit": UNIT, "cores": 1, "kind": "reference",
+                    "sample": f"{len(cols)} columns of this workload stratified by |J_k| (8 "
+                              f"equal-count strata, seeded), reference SPAI_Column loop, "
+                              f"1 thread ({secs:.1f} s)"}
             else:
-                cols = 48
-                rate, secs = oracle_port_rate(w, cols)
+                rate, secs = oracle_port_rate(w, cols[:100])
                 out["cpu_baseline"] = {
                     "value": rate, "unit": UNIT, "cores": 1, "kind": "port",
-                    "sample": f"columns [0, {cols}) via the oracle restatement ({secs:.1f} s)"}
+                    "sample": f"100 stratified columns via the oracle restatement ({secs:.1f} s)"}
         except Exception as exc:  # the baseline is reported, never the target
             out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
                                    "sample": f"failed: {exc}"}

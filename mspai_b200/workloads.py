@@ -283,20 +283,19 @@ def block27(N: int = 40, rho: float = 10.0, probing: bool = True) -> Workload:
 
 # ---------------------------------------------------------------- Matrix Market
 def write_mm(path: str, M: sp.spmatrix, pattern: bool = False) -> None:
-    """Matrix Market coordinate writer ('general'; 'pattern' drops values)."""
+    """Matrix Market coordinate writer ('general'; 'pattern' drops values),
+    entries in column order, values with 17 significant digits (exact)."""
+    import pandas as pd
     C = sp.coo_matrix(M)
     order = np.lexsort((C.row, C.col))
-    r = C.row[order] + 1
-    c = C.col[order] + 1
+    cols = {"r": C.row[order].astype(np.int64) + 1, "c": C.col[order].astype(np.int64) + 1}
+    if not pattern:
+        cols["v"] = C.data[order]
     with open(path, "w") as f:
         kind = "pattern" if pattern else "real"
         f.write(f"%%MatrixMarket matrix coordinate {kind} general\n")
         f.write(f"{C.shape[0]} {C.shape[1]} {C.nnz}\n")
-        if pattern:
-            np.savetxt(f, np.stack([r, c], 1), fmt="%d %d")
-        else:
-            v = C.data[order]
-            np.savetxt(f, np.column_stack([r, c, v]), fmt="%d %d %.17g")
+        pd.DataFrame(cols).to_csv(f, sep=" ", header=False, index=False, float_format="%.17g")
 
 
 def read_mm(path: str) -> sp.csc_matrix:
