@@ -107,6 +107,9 @@ typedef struct {
                          zero.  Used to shard the columns over several GPUs;
                          not in the reference (its column ranges come from
                          the MPI distribution, src/Distribution.cpp:48-71) */
+    int32_t keep_factors; /* 1: keep every column's triangular factor R in the
+                         handle (fixed scalar patterns) for mspai_adjoint's
+                         gbar term; not in the reference (0)              */
 } mspai_params;
 
 /* Per-setup statistics. */
@@ -197,19 +200,32 @@ int mspai_column_info(mspai_handle* h, double* resnorm, int32_t* steps, int32_t*
 int mspai_get_stats(mspai_handle* h, mspai_stats* s);
 
 /*
- * Adjoint of the last fixed-pattern scalar setup (ns == 0) for the loss
+ * Adjoint of the last setup for the loss
  *     L = ||C M - B||_F^2 + sum_k gbar_k^T m_k        (gbar optional)
- * where M solves the setup's least-squares problems at its fixed pattern.
- * C and B must be the matrices of that setup (B NULL: B = I).  Writes
- * dL/dC at the nonzeros of C (C's order, C->nnz values) and, if dB_values is
- * not NULL, dL/dB at the nonzeros of B; *loss receives L.  gbar_values
- * (nnz(M) values in M's order) may be NULL.  All value arrays live where
- * `mem` says.  The gradient is computed from the cached R of every column
- * (two triangular solves), never from a stored Q.
+ * at the pattern the setup chose (fixed, or the final pattern of the pattern
+ * updates: the pattern is a discrete choice and carries no gradient), for
+ * scalar and block setups (gbar: scalar setups only).  C and B must be the
+ * matrices of that setup (B NULL: B = I).  Writes dL/dC at the nonzeros of C
+ * (C's order, C->nnz values) and, if dB_values is not NULL, dL/dB at the
+ * nonzeros of B; *loss receives L.  gbar_values (nnz(M) values in M's order)
+ * may be NULL.  All value arrays live where `mem` says.  The residual term
+ * needs no solve (M is stationary); the gbar term needs
+ * lambda_k = R_k^-1 R_k^-T gbar_k: from the R that the setup kept
+ * (keep_factors; refined in FP64 when R is FP32), else from R recomputed in
+ * FP64.  Q is never stored.  Not in the reference.
  */
 int mspai_adjoint(mspai_handle* h, const mspai_csc* C, const mspai_csc* B,
                   const double* gbar_values, double* dC_values, double* dB_values,
                   double* loss, int32_t mem);
+
+/*
+ * mspai_adjoint for L = w ||C M - B||_F^2 + sum_k gbar_k^T m_k with the
+ * residual weight w = residual_weight (0: the sensitivity of gbar . M alone,
+ * the backward pass of M as a function of C and B).
+ */
+int mspai_adjoint_weighted(mspai_handle* h, const mspai_csc* C, const mspai_csc* B,
+                           const double* gbar_values, double residual_weight,
+                           double* dC_values, double* dB_values, double* loss, int32_t mem);
 
 /* Last error message of the handle ("" if none). */
 const char* mspai_last_error(mspai_handle* h);

@@ -36,7 +36,8 @@ class mspai_params(ctypes.Structure):
                 ("rho", ctypes.c_double), ("bs", ctypes.c_int32), ("target", ctypes.c_int32),
                 ("probing", ctypes.c_int32), ("prec", ctypes.c_int32), ("refine", ctypes.c_int32),
                 ("batched", ctypes.c_int32), ("verbose", ctypes.c_int32),
-                ("col_begin", ctypes.c_int32), ("col_end", ctypes.c_int32)]
+                ("col_begin", ctypes.c_int32), ("col_end", ctypes.c_int32),
+                ("keep_factors", ctypes.c_int32)]
 
 
 class mspai_stats(ctypes.Structure):
@@ -62,7 +63,7 @@ EXPORTED = [
     "mspai_default_params", "mspai_validate_params", "mspai_create", "mspai_setup",
     "mspai_apply", "mspai_tune",
     "mspai_result_nnz", "mspai_result_copy", "mspai_column_info", "mspai_get_stats",
-    "mspai_adjoint", "mspai_last_error", "mspai_free", "mspai_version",
+    "mspai_adjoint", "mspai_adjoint_weighted", "mspai_last_error", "mspai_free", "mspai_version",
     "mspai_matrix_view", "mspai_matrix_free", "mspai_mm_read", "mspai_mm_write",
     "mspai_probing_assemble", "mspai_pattern_generate", "mspai_row_structure",
     "mspai_measure_fma_peak", "mspai_setup_fixed_noalloc", "mspai_block_pattern_generate",
@@ -108,6 +109,9 @@ def load() -> ctypes.CDLL:
     lib.mspai_adjoint.argtypes = [V, P(mspai_csc), P(mspai_csc), V, V, V,
                                   P(ctypes.c_double), ctypes.c_int32]
     lib.mspai_adjoint.restype = I
+    lib.mspai_adjoint_weighted.argtypes = [V, P(mspai_csc), P(mspai_csc), V, ctypes.c_double, V,
+                                           V, P(ctypes.c_double), ctypes.c_int32]
+    lib.mspai_adjoint_weighted.restype = I
     lib.mspai_last_error.argtypes = [V]
     lib.mspai_last_error.restype = ctypes.c_char_p
     lib.mspai_free.argtypes = [V]

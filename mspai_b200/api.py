@@ -49,6 +49,7 @@ class Options:
     verbose: int = 0
     col_begin: int = 0         # solve only columns [col_begin, col_end) (0, 0: all)
     col_end: int = 0
+    keep_factors: bool = False  # keep every column's R for the adjoint's gbar term
 
     def to_c(self) -> mspai_params:
         p = mspai_params()
@@ -56,6 +57,7 @@ class Options:
         for f in ("ep", "mn", "ns", "um", "hs", "cs", "qr", "ch", "fg", "pk", "pm", "schur",
                   "rho", "bs", "target", "probing", "refine", "verbose", "col_begin", "col_end"):
             setattr(p, f, getattr(self, f))
+        p.keep_factors = 1 if self.keep_factors else 0
         p.prec = _lib.PREC_FP64 if self.prec == "fp64" else _lib.PREC_MIXED
         p.batched = 1 if self.batched else 0
         return p
@@ -267,8 +269,9 @@ class Handle:
         }
 
     def adjoint(self, C: MatrixLike, B: Optional[MatrixLike] = None,
-                gbar: Optional[np.ndarray] = None):
-        """Gradient of ||C M - B||_F^2 + gbar . M w.r.t. the nonzeros of C and B.
+                gbar: Optional[np.ndarray] = None, residual_weight: float = 1.0):
+        """Gradient of w ||C M - B||_F^2 + gbar . M (w = residual_weight) with
+        respect to the nonzeros of C and B, at the last setup's pattern.
 
         Returns (dC, dB, loss) as host arrays in C's / B's nonzero order."""
         sc = _Staged(C, False)
@@ -278,14 +281,32 @@ class Handle:
         g = None
         if gbar is not None:
             g = np.ascontiguousarray(gbar, dtype=np.float64)
+            if g.size != self.nnz():
+                raise ValueError(f"gbar has {g.size} values, M has {self.nnz()}")
         loss = ctypes.c_double()
-        rc = self._lib.mspai_adjoint(self._h, ctypes.byref(sc.c),
-                                     ctypes.byref(sb.c) if sb else None,
-                                     None if g is None else g.ctypes.data, dC.ctypes.data,
-                                     None if dB is None else dB.ctypes.data,
-                                     ctypes.byref(loss), MEM_HOST)
+        rc = self._lib.mspai_adjoint_weighted(self._h, ctypes.byref(sc.c),
+                                              ctypes.byref(sb.c) if sb else None,
+                                              None if g is None else g.ctypes.data,
+                                              float(residual_weight), dC.ctypes.data,
+                                              None if dB is None else dB.ctypes.data,
+                                              ctypes.byref(loss), MEM_HOST)
         self._check(rc)
         return dC[:sc.c.nnz], (dB[:sb.c.nnz] if dB is not None else None), float(loss.value)
+
+    def adjoint_device(self, C: "DeviceCSC", dC, B: Optional["DeviceCSC"] = None, dB=None,
+                       gbar=None, residual_weight: float = 1.0) -> float:
+        """mspai_adjoint_weighted with every value array in device memory: C and
+        B on the GPU, dC / dB / gbar float64 CUDA tensors (dC: C's nnz
+        values).  Returns the loss."""
+        sc = _Staged(C, False)
+        sb = _Staged(B, False) if B is not None else None
+        loss = ctypes.c_double()
+        rc = self._lib.mspai_adjoint_weighted(
+            self._h, ctypes.byref(sc.c), ctypes.byref(sb.c) if sb else None,
+            None if gbar is None else gbar.data_ptr(), float(residual_weight), dC.data_ptr(),
+            None if dB is None else dB.data_ptr(), ctypes.byref(loss), MEM_DEVICE)
+        self._check(rc)
+        return float(loss.value)
 
 
 def measure_fma_peak(device: int = 0, fp64: bool = False) -> float:

@@ -1189,6 +1189,20 @@ __device__ bool fixed_solve_column(const CtaGroup<NT>& g, FixShared<T>& fs, cons
         PHASE_MARK(5);
     }
 
+    // the caller keeps R (packed by columns) for the adjoint
+    if (out.rstore) {
+        T* dst = static_cast<T*>(out.rstore) + out.roff[col];
+        for (int t = tid; t < n * (n + 1) / 2; t += NT) {
+            int j = static_cast<int>((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
+            while (j * (j + 1) / 2 > t)
+                j--;
+            while ((j + 1) * (j + 2) / 2 <= t)
+                j++;
+            const int i = t - j * (j + 1) / 2;
+            dst[t] = Rst[fix_rs(i, n) + (j - i)];
+        }
+    }
+
     // R in global memory: move it into the skyline's region, dead after the QR
     if (!r_in_smem && reinterpret_cast<char*>(sky + r_elems) <= arena_base + arena_cap) {
         for (int i = tid; i < r_elems; i += NT)

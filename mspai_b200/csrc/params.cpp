@@ -36,6 +36,7 @@ extern "C" void mspai_default_params(mspai_params* p)
     p->verbose = 0;
     p->col_begin = 0;
     p->col_end = 0;
+    p->keep_factors = 0;
 }
 
 static int fail(char* msg, int len, const char* text)

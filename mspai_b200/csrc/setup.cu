@@ -91,6 +91,9 @@ struct mspai_handle {
     bool rows_valid = false;
     DevBuf rkeys, rslot_rep, rslot_of, rrep;  // reuse table
     DevBuf rglob;  // per-CTA areas for R of the fixed-pattern solver
+    DevBuf rstore, roff;  // R of every column (keep_factors), packed by columns
+    bool r_valid = false;
+    int r_elem = 8;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t evb[2 * kKernels] = {};
     // result description
@@ -530,6 +533,24 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     out.steps = h->steps.as<int32_t>();
     out.status = h->status.as<int32_t>();
     out.work = h->work.as<double>();
+    // ---- the columns' triangular factors for the adjoint (fixed scalar patterns)
+    h->r_valid = false;
+    if (prm->keep_factors && !compact) {
+        CUDA_TRY(h, h->cap_len.ensure(sizeof(int32_t) * std::max(n, 1)));
+        CUDA_TRY(h, h->roff.ensure(sizeof(int64_t) * (n + 1)));
+        h->launches += 5;
+        CUDA_TRY(h, mspai::launch_tri_len(pb.pptr, n, h->cap_len.as<int32_t>(), st));
+        CUDA_TRY(h, mspai::launch_scan_lengths(h->cap_len.as<int32_t>(), n, h->roff.as<int64_t>(),
+                                               h->scan_tmp.as<int64_t>(), st));
+        int64_t rtotal = 0;
+        CUDA_TRY(h, cudaMemcpyAsync(&rtotal, h->roff.as<int64_t>() + n, sizeof(int64_t),
+                                    cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(h, cudaStreamSynchronize(st));
+        CUDA_TRY(h, h->rstore.ensure(static_cast<size_t>(elem) * std::max<int64_t>(rtotal, 1)));
+        out.rstore = h->rstore.p;
+        out.roff = h->roff.as<int64_t>();
+        h->r_elem = elem;
+    }
 
     // ---- plan and bucket
     CUDA_TRY(h, h->E.ensure(sizeof(int32_t) * std::max(nprob, 1)));
@@ -540,8 +561,9 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     CUDA_TRY(h, mspai::launch_plan(pb.cptr, pb.pptr, pb.pidx, nprob, bs, h->E.as<int32_t>(),
                                    h->nk.as<int32_t>(), st));
     // ---- reuse of identical problems (-cs / -ch): fixed scalar patterns
-    const bool reuse =
-        (prm->cs > 0 || prm->ch > 0) && !adaptive && bs == 1 && prm->batched && !partial;
+    // (not with keep_factors: a reused column has no factor of its own)
+    const bool reuse = (prm->cs > 0 || prm->ch > 0) && !adaptive && bs == 1 && prm->batched &&
+                       !partial && !prm->keep_factors;
     int32_t* drep = nullptr;
     if (reuse) {
         const int max_keys = prm->cs > 0 ? prm->cs : nprob;
@@ -778,6 +800,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     h->stats.kernel_launches = h->launches;
     h->last_params = *prm;
     h->have_result = true;
+    h->r_valid = out.rstore != nullptr;
     return MSPAI_OK;
 }
 
@@ -979,14 +1002,24 @@ extern "C" int mspai_adjoint(mspai_handle* h, const mspai_csc* C, const mspai_cs
                              const double* gbar_values, double* dC_values, double* dB_values,
                              double* loss, int32_t mem)
 {
+    return mspai_adjoint_weighted(h, C, B, gbar_values, 1.0, dC_values, dB_values, loss, mem);
+}
+
+extern "C" int mspai_adjoint_weighted(mspai_handle* h, const mspai_csc* C, const mspai_csc* B,
+                                      const double* gbar_values, double residual_weight,
+                                      double* dC_values, double* dB_values, double* loss,
+                                      int32_t mem)
+{
     if (!h || !h->have_result)
         return h ? set_err(h, MSPAI_ERR_STATE, "no setup result") : MSPAI_ERR_STATE;
-    if (!h->fixed_pattern)
-        return set_err(h, MSPAI_ERR_STATE,
-                       "the adjoint needs a fixed-pattern setup (ns = 0): the pattern update "
-                       "is not differentiable");
+    const int bs = std::max(1, h->last_params.bs);
+    if (gbar_values && bs != 1)
+        return set_err(h, MSPAI_ERR_PARAM,
+                       "gbar needs a scalar setup (bs = 1): block columns have no gbar term");
     if (!C || !dC_values)
         return set_err(h, MSPAI_ERR_PARAM, "C and dC are required");
+    if (!std::isfinite(residual_weight))
+        return set_err(h, MSPAI_ERR_PARAM, "the residual weight must be finite");
     if (C->ncols != h->n)
         return set_err(h, MSPAI_ERR_INPUT, "C does not match the last setup");
     if (B && (B->ncols != h->n || B->nrows != C->nrows))
@@ -994,6 +1027,7 @@ extern "C" int mspai_adjoint(mspai_handle* h, const mspai_csc* C, const mspai_cs
     CUDA_TRY(h, cudaSetDevice(h->device));
     cudaStream_t st = h->stream;
     const int n = h->n;
+    const int nprob = h->nprob;
     Problem pb{};
     pb.n = n;
     pb.nrows = C->nrows;
@@ -1005,16 +1039,22 @@ extern "C" int mspai_adjoint(mspai_handle* h, const mspai_csc* C, const mspai_cs
         CUDA_TRY(h, stage(h->bidx, B->rowidx, B->nnz, B->mem, st, &pb.bidx));
         CUDA_TRY(h, stage(h->bval, B->values, B->nnz, B->mem, st, &pb.bval));
     }
-    pb.pptr = h->res_ptr;
-    pb.pidx = h->res_idx;
-    pb.bs = 1;
+    pb.bs = bs;
     mspai::AdjointIO io{};
     io.mptr = h->res_ptr;
+    io.midx = h->res_idx;
+    io.mval = h->res_val;
+    io.wres = residual_weight;
     DevBuf gbuf, dcbuf, dbbuf, lossbuf, cnt;
     if (gbar_values) {
         const double* gp = nullptr;
         CUDA_TRY(h, stage(gbuf, gbar_values, static_cast<size_t>(h->nnz_m), mem, st, &gp));
         io.gbar = gp;
+        if (h->r_valid) {
+            io.rstore = h->rstore.p;
+            io.roff = h->roff.as<int64_t>();
+            io.r_elem = h->r_elem;
+        }
     }
     if (mem == MSPAI_MEM_DEVICE) {
         io.dC = dC_values;
@@ -1031,29 +1071,29 @@ extern "C" int mspai_adjoint(mspai_handle* h, const mspai_csc* C, const mspai_cs
     CUDA_TRY(h, cudaMemsetAsync(io.dC, 0, sizeof(double) * C->nnz, st));
     if (io.dB)  // entries of columns outside the setup's range stay zero
         CUDA_TRY(h, cudaMemsetAsync(io.dB, 0, sizeof(double) * B->nnz, st));
-    CUDA_TRY(h, lossbuf.ensure(sizeof(double) * std::max(n, 1)));
+    CUDA_TRY(h, lossbuf.ensure(sizeof(double) * std::max(nprob, 1)));
     io.loss = lossbuf.as<double>();
-    CUDA_TRY(h, cudaMemsetAsync(io.loss, 0, sizeof(double) * std::max(n, 1), st));
-    // sizes
+    CUDA_TRY(h, cudaMemsetAsync(io.loss, 0, sizeof(double) * std::max(nprob, 1), st));
+    // sizes: entries and pattern length of each problem column at the result's pattern
     CUDA_TRY(h, cnt.ensure(64 * sizeof(int32_t)));
     int32_t* dcnt = cnt.as<int32_t>();
     CUDA_TRY(h, cudaMemsetAsync(dcnt, 0, 64 * sizeof(int32_t), st));
-    CUDA_TRY(h, h->E.ensure(sizeof(int32_t) * std::max(n, 1)));
-    CUDA_TRY(h, h->nk.ensure(sizeof(int32_t) * std::max(n, 1)));
-    CUDA_TRY(h, h->lists.ensure(sizeof(int32_t) * 3 * static_cast<size_t>(std::max(n, 1))));
+    CUDA_TRY(h, h->E.ensure(sizeof(int32_t) * std::max(nprob, 1)));
+    CUDA_TRY(h, h->nk.ensure(sizeof(int32_t) * std::max(nprob, 1)));
+    CUDA_TRY(h, h->lists.ensure(sizeof(int32_t) * 3 * static_cast<size_t>(std::max(nprob, 1))));
     h->launches++;
-    CUDA_TRY(h, mspai::launch_plan(pb.cptr, pb.pptr, pb.pidx, n, 1, h->E.as<int32_t>(),
-                                   h->nk.as<int32_t>(), st));
+    CUDA_TRY(h, mspai::launch_adjoint_plan(pb.cptr, io.mptr, io.midx, nprob, bs,
+                                           h->E.as<int32_t>(), h->nk.as<int32_t>(), st));
     // the columns of the last setup
     const int alo = h->last_params.col_begin;
-    const int ahi = h->last_params.col_end > 0 ? h->last_params.col_end : n;
+    const int ahi = h->last_params.col_end > 0 ? h->last_params.col_end : nprob;
     BucketRule rule{};
     rule.single_bucket = 0;
     rule.elem_bytes = 8;
     rule.lo = alo;
     rule.hi = ahi;
     h->launches++;
-    CUDA_TRY(h, mspai::launch_bucket(h->E.as<int32_t>(), h->nk.as<int32_t>(), n, rule, dcnt,
+    CUDA_TRY(h, mspai::launch_bucket(h->E.as<int32_t>(), h->nk.as<int32_t>(), nprob, rule, dcnt,
                                      dcnt + 4, dcnt + 8, h->lists.as<int32_t>(), st));
     int32_t hc[16];
     CUDA_TRY(h, cudaMemcpyAsync(hc, dcnt, sizeof(hc), cudaMemcpyDeviceToHost, st));
@@ -1065,17 +1105,18 @@ extern "C" int mspai_adjoint(mspai_handle* h, const mspai_csc* C, const mspai_cs
     cap.mwmax = cap.emax / 2 + cap.nmax;
     cap.cmax = cap.emax;  // q = C lambda is kept in the rho[] area
     cap.lcand = 0;
-    cap.nrhs = 1;
+    cap.nrhs = bs;
     cap.nbmap = 0;
     const bool warp = cap.emax <= 64 && cap.nmax <= 16;
-    const size_t need = mspai::adjoint_scratch_bytes(cap, n, warp);
+    const size_t need = mspai::adjoint_scratch_bytes(cap, nprob, warp);
     CUDA_TRY(h, h->scratch.ensure(need));
     CUDA_TRY(h, cudaMemsetAsync(dcnt + 20, 0, sizeof(int32_t), st));
+    h->launches++;
     CUDA_TRY(h, mspai::launch_adjoint(pb, cap, io, alo, ahi, warp, h->scratch.as<char>(),
                                       h->scratch.bytes, dcnt + 20, st));
-    std::vector<double> hl(n);
-    if (n > 0)
-        CUDA_TRY(h, cudaMemcpyAsync(hl.data(), io.loss, sizeof(double) * n,
+    std::vector<double> hl(nprob);
+    if (nprob > 0)
+        CUDA_TRY(h, cudaMemcpyAsync(hl.data(), io.loss, sizeof(double) * nprob,
                                     cudaMemcpyDeviceToHost, st));
     if (mem == MSPAI_MEM_HOST) {
         CUDA_TRY(h, cudaMemcpyAsync(dC_values, io.dC, sizeof(double) * C->nnz,
@@ -1087,10 +1128,15 @@ extern "C" int mspai_adjoint(mspai_handle* h, const mspai_csc* C, const mspai_cs
     CUDA_TRY(h, cudaStreamSynchronize(st));
     CUDA_TRY(h, cudaGetLastError());
     if (loss) {
-        double s = 0.0;
-        for (double v : hl)
-            s += v;
-        *loss = s;
+        // compensated (Neumaier) sum: the columns' losses are often nearly
+        // equal, and a plain running sum lets their rounding errors add up
+        double s = 0.0, comp = 0.0;
+        for (double v : hl) {
+            const double t = s + v;
+            comp += std::fabs(s) >= std::fabs(v) ? (s - t) + v : (v - t) + s;
+            s = t;
+        }
+        *loss = s + comp;
     }
     gbuf.release();
     dcbuf.release();

@@ -211,6 +211,24 @@ __global__ void finish_ptr_kernel(int64_t* __restrict__ ptr, int n, const int32_
         ptr[n] = (n > 0) ? ptr[n - 1] + len[n - 1] : 0;
 }
 
+// entries of a packed triangle of |P(:, k)|: n_k (n_k + 1) / 2
+__global__ void tri_len_kernel(const int64_t* __restrict__ pptr, int n, int32_t* __restrict__ len)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int64_t nk = pptr[k + 1] - pptr[k];
+        len[k] = static_cast<int32_t>(nk * (nk + 1) / 2);
+    }
+}
+
+cudaError_t launch_tri_len(const int64_t* pptr, int n, int32_t* len, cudaStream_t st)
+{
+    if (n <= 0)
+        return cudaSuccess;
+    int blocks = std::min((n + 255) / 256, num_sms() * 8);
+    tri_len_kernel<<<blocks, 256, 0, st>>>(pptr, n, len);
+    return cudaGetLastError();
+}
+
 // capacity of scalar column sc: bs * (|P(:, sc / bs)| + grow) entries
 __global__ void capacity_len_kernel(const int64_t* __restrict__ pptr, int n, int bs, int grow,
                                     int32_t* __restrict__ len)

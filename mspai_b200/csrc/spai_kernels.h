@@ -84,6 +84,8 @@ cudaError_t launch_fixed_solve(int elem_bytes, int arena_bytes, const Problem& p
                                cudaStream_t st, int* grid_out);
 cudaError_t launch_scan_lengths(const int32_t* len, int n, int64_t* ptr, int64_t* tmp,
                                 cudaStream_t st);
+// len[k] = |P(:, k)| (|P(:, k)| + 1) / 2 (packed triangles of the kept R)
+cudaError_t launch_tri_len(const int64_t* pptr, int n, int32_t* len, cudaStream_t st);
 cudaError_t launch_capacity_len(const int64_t* pptr, int n, int bs, int grow, int32_t* len,
                                 cudaStream_t st);
 cudaError_t launch_compact(const int64_t* cap_ptr, const int32_t* cidx, const double* cval,
@@ -109,15 +111,25 @@ cudaError_t launch_reuse_keys(const Problem& pb, int nprob, const ReuseTable& t,
                               int32_t* nreused, cudaStream_t st);
 cudaError_t launch_reuse_copy(const int32_t* rep, int nprob, const Output& out, cudaStream_t st);
 
-// Adjoint of the fixed-pattern setup (adjoint.cu).
+// Adjoint of the setup (adjoint.cu): problem columns read their pattern and
+// solutions from the result M.
 struct AdjointIO {
-    const int64_t* mptr;  // M's pattern pointers (== P of the setup)
-    const double* gbar;   // nnz(M) or null
+    const int64_t* mptr;  // M (the setup's result): n + 1 pointers, scalar columns
+    const int32_t* midx;
+    const double* mval;
+    const double* gbar;   // nnz(M) or null (scalar setups)
+    const void* rstore;   // R kept by the setup (packed by columns) or null
+    const int64_t* roff;
+    int r_elem;           // 4 or 8: the element size of rstore
+    double wres;          // weight of the residual term ||C M - B||_F^2
     double* dC;           // nnz(C), zero on entry
     double* dB;           // nnz(B) or null
-    double* loss;         // per column
+    double* loss;         // per problem column
 };
-// columns [lo, hi) of the last setup
+// E[k], nk[k] of problem column k from the result's pattern
+cudaError_t launch_adjoint_plan(const int64_t* cptr, const int64_t* mptr, const int32_t* midx,
+                                int nprob, int bs, int32_t* E, int32_t* nk, cudaStream_t st);
+// problem columns [lo, hi) of the last setup
 cudaError_t launch_adjoint(const Problem& pb, const Caps& cap, const AdjointIO& io, int lo,
                            int hi, bool warp, char* scratch, size_t scratch_bytes,
                            int32_t* counter, cudaStream_t st);

@@ -68,6 +68,10 @@ struct Output {
     double* work;          // 3 per column: folded flops, dense-equivalent
                            // flops, gather bytes (accumulated over steps)
     int write_idx;         // 1: write oidx
+    // optional (fixed scalar patterns): R of column k packed by columns,
+    // R(i, j) at rstore + roff[k] + j (j + 1) / 2 + i, in the solve's precision
+    void* rstore;
+    const int64_t* roff;
 };
 
 // Capacities of one problem slot.
@@ -650,6 +654,19 @@ __device__ __forceinline__ double block_rho_term(double* Gm, const double* N, in
     return term;
 }
 
+// Copies R (n x n upper triangle of the view) packed by columns to dst.
+template <class T, class G>
+__device__ void group_store_r(const G& g, RView<T> R, int n, T* dst)
+{
+    if (R.ld == 0) {
+        for (int t = g.rank(); t < n * (n + 1) / 2; t += G::kSize)
+            dst[t] = R.p[t];
+    }
+    else {
+        group_pack_r<T>(g, R.p, R.ld, n, dst);
+    }
+}
+
 // Solves problem column `col` (scalar column col, or block column col when
 // pb.bs > 1; then the bs scalar columns bs*col .. bs*col+bs-1 of M share J,
 // I and one QR, with bs right-hand sides).  Results go to `out`.
@@ -928,6 +945,8 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
                 rv = RView<T>{rp, 0};
                 rhs_s = rh;
             }
+            if (out.rstore && pb.ns == 0 && bs == 1)
+                group_store_r<T>(g, rv, n, static_cast<T*>(out.rstore) + out.roff[col]);
             PHASE_MARK(3);
             for (int c = 0; c < nrhs; c++)
                 sing |= group_back_substitute_blocked<T>(g, rv, n, rhs_s + static_cast<size_t>(c) * ldr,
@@ -950,6 +969,8 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
                 rhs_s = rh;
                 ldr = n;
             }
+            if (out.rstore && pb.ns == 0 && bs == 1)
+                group_store_r<T>(g, rv, n, static_cast<T*>(out.rstore) + out.roff[col]);
             PHASE_MARK(3);
             for (int c = 0; c < nrhs; c++)
                 sing |= group_back_substitute_blocked<T>(g, rv, n, rhs_s + static_cast<size_t>(c) * ldr,
@@ -957,6 +978,8 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
         }
         else {
             group_householder<T>(g, W, ld, mw, n, nrhs);
+            if (out.rstore && pb.ns == 0 && bs == 1)
+                group_store_r<T>(g, RView<T>{W, ld}, n, static_cast<T*>(out.rstore) + out.roff[col]);
             for (int c = 0; c < nrhs; c++)
                 sing |= group_back_substitute<T>(g, W, ld, n, rhs + static_cast<size_t>(c) * ld,
                                                  s.x + static_cast<size_t>(c) * n);
