@@ -54,6 +54,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="skip the sub-lines of the other benchmark workloads")
+    ap.add_argument("--strong", action="store_true",
+                    help="strong scaling: one n-column problem split over the ranks "
+                         "(work-balanced column ranges), M assembled in HBM on every rank "
+                         "by NCCL inside the timed region")
     return ap.parse_args()
 
 
@@ -165,9 +171,14 @@ def write_subproblem(w, cols, directory):
     Psub = sp.csc_matrix((np.ones(len(prow)), (prow, pcol)), shape=(n, n))
     W.write_mm(os.path.join(directory, "A.mtx"), Asub)
     W.write_mm(os.path.join(directory, "P.mtx"), Psub, pattern=True)
+    if w.Ce is not None:
+        # probing rows: only the kept columns are ever read
+        D = sp.diags(keep.astype(np.float64))
+        W.write_mm(os.path.join(directory, "Ce.mtx"), sp.csr_matrix(w.Ce) @ D)
+        W.write_mm(os.path.join(directory, "Be.mtx"), sp.csr_matrix(w.Be) @ D)
 
 
-def reference_step_times(directory, chunks, reps):
+def reference_step_times(directory, chunks, reps, ref_args=("A.mtx", "P.mtx", "-1", "-ns", "0")):
     """Runs the reference's SPAI_Column loop, one process per chunk of columns
     (OPENBLAS_NUM_THREADS=1), `reps` passes after one read of the inputs.
     Returns the per-pass wall time of the slowest process (s), per pass."""
@@ -178,7 +189,7 @@ def reference_step_times(directory, chunks, reps):
         np.savetxt(cf, np.asarray(chunk, dtype=np.int64), fmt="%d")
         tf = os.path.join(directory, f"t_{p}.json")
         jobs.append((subprocess.Popen(
-            [REF_DRIVER, "A.mtx", "P.mtx", "-1", "-ns", "0", "-colfile", cf, "-repeat", str(reps),
+            [REF_DRIVER, *ref_args, "-colfile", cf, "-repeat", str(reps),
              "-time", tf, "-out", f"M_{p}.mtx"], cwd=directory, env=env,
             stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL), tf))
     per_proc = []
@@ -285,6 +296,196 @@ def bench_reference(args):
     return 0
 
 
+# ------------------------------------------------------------------ other workloads
+L2_FLUSH_BYTES = 256 << 20  # twice the 126 MB L2
+
+
+def timed_steps(fn, stream, steps, warmup, flush):
+    """Device ms of each of `steps` calls of fn (CUDA events on `stream`),
+    after `warmup` calls; L2 flushed (a 256 MB write) before each timed call,
+    outside its events."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    out = []
+    for _ in range(steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return out
+
+
+def dominant_roofline(st, peak32, fixed: bool):
+    """Roofline entry of the setup's dominant bucket (largest kernel time):
+    folded FLOPs of its launch / its event time, against the FP32 FMA peak."""
+    b = int(np.argmax(st["kernel_ms"]))
+    kms = st["kernel_ms"][b]
+    achieved = st["bucket_flops"][b] / (kms * 1e-3) / 1e12 if kms > 0 else None
+    names = (["warp_solve_kernel", "fixed_solve_kernel (first launch)",
+              "fixed_solve_kernel (large arena)", "cta_solve_kernel"] if fixed else
+             ["warp_solve_kernel", "cta_solve_kernel (W in shared memory)",
+              "cta_solve_kernel (W in global memory)", "cta_solve_kernel"])
+    return {"bound": "fp32", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
+            "frac": (achieved / peak32) if achieved else None, "traffic": None,
+            "kernel": names[b],
+            "kernel_ms": kms, "flops_per_launch": st["bucket_flops"][b],
+            "peak_source": "measured FP32 FMA probe (mspai_measure_fma_peak)"}
+
+
+def reference_sample_rate(w, cols, ref_args, restrict: bool):
+    """Columns/s of the reference's column loop on one core over `cols`
+    (one process, one pass after reading the inputs)."""
+    import scipy.sparse as sp
+    from mspai_b200 import workloads as W
+    with tempfile.TemporaryDirectory() as d:
+        if restrict:
+            write_subproblem(w, cols, d)
+        else:
+            W.write_mm(os.path.join(d, "A.mtx"), sp.csc_matrix(w.A))
+        secs = reference_step_times(d, [cols], 1, ref_args)[-1]
+    return len(cols) / secs, secs
+
+
+def bench_workloads(args, h, stream, world, rank, peak32):
+    """Sub-lines for the convection-diffusion (adaptive), anisotropic probing
+    (fixed pattern + adjoint) and block 27-point (block updates + probing +
+    adjoint) workloads: columns/s with inputs resident in HBM, the dominant
+    kernel's roofline, and the reference's one-core rate on a seeded sample."""
+    import torch
+    import scipy.sparse as sp
+    import mspai_b200 as mb
+    from mspai_b200 import workloads as W
+
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=stream.device)
+    steps = max(1, min(args.steps, 3))
+    warm = 3
+    lines = {}
+    do_cpu = rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_DRIVER)
+
+    def rate(ms_list, n_cols):
+        ms = max_over_ranks(float(np.median(ms_list)), world)
+        return world * n_cols / (ms * 1e-3), ms
+
+    # ---- 3-D convection-diffusion 48^3, adaptive (-ep 0.4 -ns 5 -mn 5 -um 1)
+    w = W.convdiff3d(48)
+    dA = mb.DeviceCSC.from_scipy(w.A)
+    dP = mb.DeviceCSC.from_scipy(w.P, pattern=True)
+    ad = dict(ep=0.4, ns=5, mn=5, um=1)
+    mixed = mb.Options(prec="mixed", **ad)
+    ms = timed_steps(lambda: h.setup(dA, dP, options=mixed), stream, steps, warm, flush)
+    value, mms = rate(ms, w.n)
+    st = h.stats()
+    _, stp, _ = h.column_info()
+    plain = mb.Options(prec="fp64", batched=False, **ad)
+    pms = timed_steps(lambda: h.setup(dA, dP, options=plain), stream, 1, 1, flush)
+    pvalue, pms1 = rate(pms, w.n)
+    line = {"workload": "convection-diffusion 48^3 (n=110,592), adaptive -ep 0.4 -ns 5 -mn 5 "
+                        "-um 1, start pattern diagonal", "value": value, "unit": UNIT,
+            "ms_per_step": mms, "steps": steps, "warmup": warm,
+            "mean_ls_solves_per_column": float(np.mean(stp)),
+            "plain_fp64": {"value": pvalue, "ms_per_step": pms1, "speedup_of_mixed": value / pvalue},
+            "roofline": dominant_roofline(st, peak32, fixed=False),
+            "l2": "flushed before each step (256 MB write)"}
+    if do_cpu:
+        cols = np.arange(w.n)
+        r, secs = reference_sample_rate(w, cols, ["A.mtx", "-1", "-1", "-ep", "0.4", "-ns", "5",
+                                                  "-mn", "5", "-um", "1"], restrict=False)
+        line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": 1, "kind": "reference",
+                                "sample": f"all {w.n} columns, reference column loop with "
+                                          f"pattern updates, 1 thread ({secs:.1f} s)"}
+    lines["convdiff48_adaptive"] = line
+    del dA, dP
+
+    # ---- anisotropic 1024^2 with two probing rows, rho 10: forward + adjoint
+    rho = 10.0
+    w = W.aniso2d_probing(1024, kinds=("ones", "alt"), rho=rho)
+    C, B = mb.assemble_probing(w.A, w.Ce, w.Be, rho)
+    dC = mb.DeviceCSC.from_scipy(C)
+    dB = mb.DeviceCSC.from_scipy(B)
+    dP = mb.DeviceCSC.from_scipy(w.P, pattern=True)
+    fwd = mb.Options(ns=0, prec="mixed", probing=1, rho=rho)
+    ms = timed_steps(lambda: h.setup(dC, dP, B=dB, options=fwd), stream, steps, warm, flush)
+    value, fms = rate(ms, w.n)
+    st = h.stats()
+    gC = torch.empty(C.nnz, dtype=torch.float64, device=stream.device)
+    gB = torch.empty(B.nnz, dtype=torch.float64, device=stream.device)
+    ams = timed_steps(lambda: h.adjoint_device(dC, gC, dB, gB), stream, steps, warm, flush)
+    avalue, ams1 = rate(ams, w.n)
+    line = {"workload": "anisotropic diffusion 1024^2 (n=1,048,576), probing rows e = ones and "
+                        "alternating, rho 10, pattern(A), fixed pattern, B = [I; rho Be]",
+            "value": value, "unit": UNIT, "ms_per_step": fms, "steps": steps, "warmup": warm,
+            "adjoint": {"value": avalue, "unit": UNIT, "ms_per_step": ams1,
+                        "what": "d||CM-B||_F^2 / d(C, B) at every nonzero (mspai_adjoint, "
+                                "device-resident C, B, dC, dB)"},
+            "forward_plus_adjoint": {"value": world * w.n / ((fms + ams1) * 1e-3), "unit": UNIT},
+            "roofline": dominant_roofline(st, peak32, fixed=True),
+            "l2": "flushed before each step (256 MB write)"}
+    if do_cpu:
+        cols = sample_columns(w.P, 100_000)
+        r, secs = reference_sample_rate(w, cols, ["A.mtx", "P.mtx", "-1", "-ns", "0", "-Ce",
+                                                  "Ce.mtx", "-Be", "Be.mtx", "-rho", "10"],
+                                        restrict=True)
+        line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": 1, "kind": "reference",
+                                "sample": f"{len(cols)} columns stratified by |J_k|, reference "
+                                          f"column loop with the probing rows, 1 thread "
+                                          f"({secs:.1f} s)"}
+    lines["aniso1024_probing"] = line
+    del dC, dB, dP, gC, gB
+
+    # ---- 27-point block stencil 40^3, bs 3, block updates, probing rho 10, adjoint
+    w = W.block27(40, rho=rho, probing=True)
+    C, B = mb.assemble_probing(w.A, w.Ce, w.Be, rho)
+    dC = mb.DeviceCSC.from_scipy(C)
+    dB = mb.DeviceCSC.from_scipy(B)
+    dpat = mb.DeviceCSC.from_scipy(sp.identity(w.n // 3, format="csc"), pattern=True)
+    # probing with pattern updates: C = [A; rho Ce] and B = [I; rho Be] given
+    # with probing = 0 (the reference's option check allows probing only
+    # without updates)
+    bo = mb.Options(prec="mixed", ep=0.4, ns=3, mn=3, bs=3)
+    ms = timed_steps(lambda: h.setup(dC, dpat, B=dB, options=bo), stream, steps, warm, flush)
+    value, bms = rate(ms, w.n)
+    st = h.stats()
+    _, stp, _ = h.column_info()
+    gC = torch.empty(C.nnz, dtype=torch.float64, device=stream.device)
+    gB = torch.empty(B.nnz, dtype=torch.float64, device=stream.device)
+    ams = timed_steps(lambda: h.adjoint_device(dC, gC, dB, gB), stream, steps, warm, flush)
+    avalue, ams1 = rate(ams, w.n)
+    line = {"workload": "27-point block stencil 40^3 x 3 (n=192,000), bs 3, block updates -ns 3 "
+                        "-mn 3 -ep 0.4, probing e = ones, rho 10",
+            "value": value, "unit": UNIT, "ms_per_step": bms, "steps": steps, "warmup": warm,
+            "mean_ls_solves_per_block_column": float(np.mean(stp[::3])),
+            "adjoint": {"value": avalue, "unit": UNIT, "ms_per_step": ams1,
+                        "what": "d||CM-B||_F^2 / d(C, B) at the final block pattern"},
+            "roofline": dominant_roofline(st, peak32, fixed=False),
+            "l2": "flushed before each step (256 MB write)"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the reference refuses probing with pattern updates: the oracle
+        # restatement of its block column loop (C++, one thread) on the same
+        # problem, probing rows included
+        from oracle import pyoracle
+        rng = np.random.default_rng(0x5A13)
+        blocks = np.sort(rng.choice(w.n // 3, size=8000, replace=False))
+        t0 = time.perf_counter()
+        pyoracle.spai_block(C, sp.identity(w.n // 3, format="csc"), 3, B=B, ns=3, mn=3, ep=0.4,
+                            block_list=blocks)
+        secs = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": 3 * len(blocks) / secs, "unit": UNIT, "cores": 1,
+                                "kind": "port",
+                                "sample": f"{len(blocks)} seeded random block columns "
+                                          f"({3 * len(blocks)} columns) through the oracle "
+                                          f"restatement of the reference's block column loop, "
+                                          f"probing rows included (the reference's option check "
+                                          f"refuses probing with updates), 1 thread, input "
+                                          f"conversion included ({secs:.1f} s)"}
+    lines["block27_40"] = line
+    return lines
+
+
 def bench_ours(args):
     import torch
     import mspai_b200 as mb
@@ -298,7 +499,7 @@ def bench_ours(args):
     dA = mb.DeviceCSC.from_scipy(w.A)
     dP = mb.DeviceCSC.from_scipy(w.P, pattern=True)
     torch.cuda.synchronize()
-    mixed = mb.Options(ns=0, prec="mixed", refine=2, batched=True)
+    mixed = mb.Options(ns=0, prec="mixed", batched=True)
     # the autotuner picks the solver's shared-memory area per CTA on a sample
     # of columns (outside the timed region)
     smem_kb = h.tune(dA, dP, options=mixed, sample_cols=min(n, 50000))
@@ -427,6 +628,9 @@ def bench_ours(args):
                       "d2h_bytes_per_step": oc.numel() * 8 + oi.numel() * 4 + ov.numel() * 8,
                       "ms_per_step": ems}
 
+    if not args.no_workloads:
+        out["workloads"] = bench_workloads(args, h, stream, world, rank, peak32)
+
     # CPU baseline: the reference's column loop on a bounded sample (one
     # process's share of the reference arm's stratified sample), 1 core
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -458,10 +662,116 @@ def bench_ours(args):
     return 0
 
 
+def bench_strong(args):
+    """One problem of n columns over all ranks (mspai_b200.distributed):
+    each rank solves its work-balanced range and the ranks assemble M in HBM
+    through NCCL (values of P's structure, all_gather_into_tensor), all inside
+    the timed region.  value = n / the slowest rank's step time."""
+    import torch
+    import mspai_b200 as mb
+    from mspai_b200 import distributed as D
+    from mspai_b200 import workloads as W
+
+    world, rank, local = dist_setup(args)
+    n = args.n
+    w = W.ragged(n, seed=BASE_SEED)          # the same problem on every rank
+    stream = torch.cuda.current_stream()
+    h = mb.Handle(local, stream=stream.cuda_stream)
+    dA = mb.DeviceCSC.from_scipy(w.A)
+    dP = mb.DeviceCSC.from_scipy(w.P, pattern=True)
+    mixed = mb.Options(ns=0, prec="mixed", batched=True)
+    group = None
+    if world == 1:
+        import datetime
+        import torch.distributed as dist
+        if not dist.is_initialized():
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            os.environ.setdefault("MASTER_PORT", "29533")
+            dist.init_process_group("nccl", rank=0, world_size=1,
+                                    timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+
+    def step(A, P):
+        ranges = D.balanced_ranges_device(D.column_work_device(A.colptr, P.colptr, P.rowidx),
+                                          world)
+        return D.sharded_setup_device(h, A, P, options=mixed, group=group, ranges=ranges)
+
+    for _ in range(max(args.warmup, 3)):
+        M = step(dA, dP)
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        M = step(dA, dP)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+    value = n / (ms * 1e-3)
+    st = h.stats()
+    # the assembled M equals a whole setup on this GPU (checked once, outside the timing)
+    h.setup(dA, dP, options=mixed)
+    Mv = torch.empty(w.P.nnz, dtype=torch.float64, device=dA.colptr.device)
+    h.result_into(None, None, Mv, device=True)
+    same = bool(torch.equal(Mv, M.values))
+    # end to end: inputs from pinned host memory, M's values back to host on rank 0
+    hA = mb.DeviceCSC.from_scipy(w.A, device="cpu", pin=True)
+    hP = mb.DeviceCSC.from_scipy(w.P, device="cpu", pattern=True, pin=True)
+    ov = torch.empty(w.P.nnz, dtype=torch.float64).pin_memory()
+    dev = dA.colptr.device
+
+    def e2e_step():
+        A = mb.DeviceCSC(hA.nrows, hA.ncols, hA.colptr.to(dev, non_blocking=True),
+                         hA.rowidx.to(dev, non_blocking=True), hA.values.to(dev, non_blocking=True))
+        P = mb.DeviceCSC(hP.nrows, hP.ncols, hP.colptr.to(dev, non_blocking=True),
+                         hP.rowidx.to(dev, non_blocking=True))
+        Mx = step(A, P)
+        if rank == 0:
+            ov.copy_(Mx.values, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    q0 = torch.cuda.Event(enable_timing=True)
+    q1 = torch.cuda.Event(enable_timing=True)
+    q0.record(stream)
+    e2e_step()
+    q1.record(stream)
+    torch.cuda.synchronize()
+    ems = max_over_ranks(q0.elapsed_time(q1), world)
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic (seeded, shapes of the ragged 1M-column configuration)",
+        "config": dict(workload_config(n), parallelism=f"column ranges over {world} ranks, "
+                       "M values all-gathered by NCCL in HBM"),
+        "clocks": clocks, "gpu_launches": int(st["kernel_launches"]) * args.steps,
+        "assembled_equals_single_setup": same,
+        "e2e": {"value": n / (ems * 1e-3), "unit": UNIT,
+                "h2d_bytes_per_step": hA.nbytes() + hP.nbytes(),
+                "d2h_bytes_per_step": ov.numel() * 8 if rank == 0 else 0, "ms_per_step": ems},
+        "roofline": None, "cpu_baseline": None,
+    }
+    h.close()
+    if rank == 0:
+        print(json.dumps(out))
+    import torch.distributed as dist
+    dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return bench_reference(args)
+    if args.strong:
+        return bench_strong(args)
     return bench_ours(args)
 
 

@@ -5,6 +5,7 @@ adjoint.  Ranges may land columns in other size buckets than the full setup
 does, so values agree within the FP64 tolerance (1e-10 relative)."""
 import numpy as np
 import pytest
+import scipy.sparse as sp
 
 import mspai_b200 as mb
 from helpers import max_rel_diff, same_pattern
@@ -87,3 +88,46 @@ def test_tuner_picks_a_candidate_and_keeps_results(h):
     h.setup(w.A, w.P, options=mb.Options(ns=0, prec="fp64"))
     after = h.result()
     assert same_pattern(after, before) and max_rel_diff(after, before) < 1e-10
+
+
+@pytest.mark.parametrize("case", ["ragged", "convdiff"])
+def test_device_sharded_setup_nccl_one_rank(h, case):
+    """sharded_setup_device through a one-rank NCCL group: ranges computed on
+    the device, M assembled in HBM by the NCCL collectives, equal to the
+    whole setup (fixed pattern: values only; adaptive: lengths, indices and
+    values)."""
+    import datetime
+    import socket
+    import torch
+    import torch.distributed as dist
+    if case == "ragged":
+        w = W.ragged(3000)
+        opts = dict(ns=0, prec="mixed")
+    else:
+        w = W.convdiff3d(8)
+        opts = dict(ep=0.4, ns=5, mn=5, prec="mixed")
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60),
+                            device_id=torch.device("cuda", 0))
+    try:
+        dA = mb.DeviceCSC.from_scipy(w.A)
+        dP = mb.DeviceCSC.from_scipy(w.P, pattern=True)
+        M = D.sharded_setup_device(h, dA, dP, options=mb.Options(**opts))
+        got = sp.csc_matrix((M.values.cpu().numpy(), M.rowidx.cpu().numpy(),
+                                    M.colptr.cpu().numpy()), shape=(w.n, w.n))
+        h.setup(w.A, w.P, options=mb.Options(**opts))
+        ref = h.result()
+        assert same_pattern(got, ref)
+        assert max_rel_diff(got, ref) == 0.0
+        # the adjoint's device form: gradients summed by NCCL
+        h.setup(dA, dP, options=mb.Options(**opts))
+        dC = torch.empty(w.A.nnz, dtype=torch.float64, device="cuda")
+        L = D.sharded_adjoint_device(h, dA, dC)
+        g, _, L2 = h.adjoint(w.A)
+        assert L == pytest.approx(L2, rel=1e-12)
+        assert np.max(np.abs(dC.cpu().numpy() - g)) <= 1e-12 * np.max(np.abs(g))
+    finally:
+        dist.destroy_process_group()

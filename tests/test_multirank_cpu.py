@@ -139,3 +139,76 @@ def test_reference_arm_prints_from_rank_zero_only():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def _gather_worker(rank, world, port, out):
+    import datetime
+    import numpy as np
+    import scipy.sparse as sp
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    from mspai_b200 import distributed as D
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        rng = np.random.default_rng(42)
+        n = 300
+        M = sp.random(n, n, density=0.03, format="csc", random_state=7)
+        M = (M + sp.identity(n)).tocsc()
+        M.sort_indices()
+        C = sp.random(n + 2, n, density=0.05, format="csc", random_state=8)
+        C = (C + sp.identity(n + 2, format="csc")[:, :n]).tocsc()
+        # work and ranges on the "device" (CPU tensors here) equal the host's
+        t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt))
+        wdev = D.column_work_device(t(C.indptr, np.int64), t(M.indptr, np.int64),
+                                    t(M.indices, np.int32))
+        whost = D.column_work(C, M)
+        ranges = D.balanced_ranges_device(wdev, world)
+        ok_work = bool(np.allclose(wdev.numpy(), whost, rtol=1e-12))
+        ok_ranges = ranges == D.balanced_ranges(whost, world)
+        lo, hi = ranges[rank]
+        # compact result: only this rank's columns are non-empty
+        lens = np.diff(M.indptr).copy()
+        mask = np.zeros(n, dtype=bool)
+        mask[lo:hi] = True
+        lens[~mask] = 0
+        cp = np.zeros(n + 1, dtype=np.int64)
+        np.cumsum(lens, out=cp[1:])
+        keep = np.repeat(mask, np.diff(M.indptr))
+        ri = M.indices[keep]
+        vv = M.data[keep]
+        gc, gr, gv = D.gather_csc_device(t(cp, np.int64), t(ri, np.int32), t(vv, np.float64),
+                                         ranges, rank)
+        G = sp.csc_matrix((gv.numpy(), gr.numpy(), gc.numpy()), shape=(n, n))
+        ok_compact = bool((G != M).nnz == 0 and np.array_equal(G.indptr, M.indptr))
+        # known structure: values in M's structure, zeros outside the range
+        vk = np.where(keep, M.data, 0.0)
+        kc, kr, kv = D.gather_csc_device(t(M.indptr, np.int64), None, t(vk, np.float64), ranges,
+                                         rank, known_structure=(t(M.indptr, np.int64),
+                                                                t(M.indices, np.int32)))
+        ok_known = bool(np.array_equal(kv.numpy(), M.data))
+        out[rank] = (ok_work, ok_ranges, ok_compact, ok_known, ranges)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_device_gather_two_ranks_gloo():
+    """The device form of the sharded setup's gather (all_reduce of column
+    lengths, padded all_gather of indices and values), on CPU tensors with
+    gloo: every rank assembles the whole M; the device work estimate and
+    ranges equal the host ones."""
+    world = 2
+    port = free_port()
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.start_processes(_gather_worker, args=(world, port, out), nprocs=world, join=True,
+                           start_method="spawn")
+        r = dict(out)
+    assert set(r) == {0, 1}
+    for rank in (0, 1):
+        ok_work, ok_ranges, ok_compact, ok_known, ranges = r[rank]
+        assert ok_work and ok_ranges and ok_compact and ok_known
+    assert r[0][4][0][1] == r[0][4][1][0] and r[0][4][1][1] == 300
