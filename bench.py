@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-resetup", action="store_true",
+                    help="skip the re-setup sub-line (kept factors, ~45 GB of R at n=1e6)")
     ap.add_argument("--no-workloads", action="store_true",
                     help="skip the sub-lines of the other benchmark workloads")
     ap.add_argument("--strong", action="store_true",
@@ -628,6 +630,49 @@ def bench_ours(args):
                       "d2h_bytes_per_step": oc.numel() * 8 + oi.numel() * 4 + ov.numel() * 8,
                       "ms_per_step": ems}
 
+    # re-setups from the kept factors: the same structure with values changed
+    # by a relative 1e-4 (seeded), alternating between the two value sets;
+    # each step starts from the previous step's solution and R
+    if not args.no_resetup:
+        keep = mb.Options(ns=0, prec="mixed", batched=True, keep_factors=True)
+        again = mb.Options(ns=0, prec="mixed", batched=True, keep_factors=True,
+                           reuse_factors=8)
+        gen = torch.Generator(device=dA.values.device).manual_seed(0x5EED + rank)
+        noise = torch.randn(dA.values.shape, generator=gen, dtype=torch.float64,
+                            device=dA.values.device)
+        dA2 = mb.DeviceCSC(dA.nrows, dA.ncols, dA.colptr, dA.rowidx,
+                           dA.values * (1.0 + 1e-4 * noise))
+        del noise
+        h.setup(dA, dP, options=keep)
+        pair = [dA2, dA]
+        for i in range(2):
+            h.setup(pair[i % 2], dP, options=again)
+        torch.cuda.synchronize()
+        r0 = torch.cuda.Event(enable_timing=True)
+        r1 = torch.cuda.Event(enable_timing=True)
+        rsteps = max(2, args.steps)
+        reused = []
+        r0.record(stream)
+        for i in range(rsteps):
+            h.setup(pair[i % 2], dP, options=again)
+            reused.append(h.stats()["factor_reuse_columns"])
+        r1.record(stream)
+        torch.cuda.synchronize()
+        rms = max_over_ranks(r0.elapsed_time(r1) / rsteps, world)
+        res_re, _, _ = h.column_info()
+        h.setup(pair[(rsteps - 1) % 2], dP, options=mixed)
+        res_fresh, _, _ = h.column_info()
+        out["resetup"] = {
+            "value": world * n / (rms * 1e-3), "unit": UNIT, "ms_per_step": rms,
+            "steps": rsteps, "speedup_over_setup": ms / rms,
+            "what": "re-setup from the kept R factors (reuse_factors 8): values of A changed "
+                    "by a relative 1e-4 (seeded), same structure",
+            "columns_from_kept_factor": int(np.median(reused)),
+            "frob_AM_minus_I_rel_diff_to_fresh": float(
+                abs(np.linalg.norm(res_re) - np.linalg.norm(res_fresh)) /
+                np.linalg.norm(res_fresh))}
+        del dA2
+
     if not args.no_workloads:
         out["workloads"] = bench_workloads(args, h, stream, world, rank, peak32)
 
@@ -675,7 +720,9 @@ def bench_strong(args):
     world, rank, local = dist_setup(args)
     n = args.n
     w = W.ragged(n, seed=BASE_SEED)          # the same problem on every rank
-    stream = torch.cuda.current_stream()
+    # one stream for torch's copies and the library's kernels
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
     h = mb.Handle(local, stream=stream.cuda_stream)
     dA = mb.DeviceCSC.from_scipy(w.A)
     dP = mb.DeviceCSC.from_scipy(w.P, pattern=True)

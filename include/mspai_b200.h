@@ -97,7 +97,9 @@ typedef struct {
                          implied; 0: arbitrary target matrix                  */
     int32_t probing;  /* 1: C has probing rows n..nrows-1 (-Ce/-Be given)    */
     int32_t prec;     /* mspai_precision (MSPAI_PREC_MIXED)                   */
-    int32_t refine;   /* FP64 refinement steps in mixed mode (2)              */
+    int32_t refine;   /* at most this many FP64 refinement steps in mixed
+                         mode (4); a column stops when its correction is
+                         below 2^-44 of its solution or stops contracting */
     int32_t batched;  /* 1: size-bucketed batched kernels (default);
                          0: the plain per-column path (one CTA per column,
                          FP64, no buckets) -- the throughput baseline         */
@@ -109,7 +111,17 @@ typedef struct {
                          the MPI distribution, src/Distribution.cpp:48-71) */
     int32_t keep_factors; /* 1: keep every column's triangular factor R in the
                          handle (fixed scalar patterns) for mspai_adjoint's
-                         gbar term; not in the reference (0)              */
+                         gbar term and for re-setups (reuse_factors) (0)   */
+    int32_t reuse_factors; /* > 0: re-setup from the kept factors.  When C, P
+                         and B have the structure of the last setup that kept
+                         its factors (keep_factors, same precision), every
+                         column of the fixed-pattern solver starts from its
+                         previous solution and R and takes at most this many
+                         FP64 refinement steps against the new values; a
+                         column that does not converge is factored again.
+                         The reference's update path keeps each column's QR
+                         across setups (src/Spai_Update.imp:45-325); 0
+                         recomputes every column (0)                       */
 } mspai_params;
 
 /* Per-setup statistics. */
@@ -130,6 +142,7 @@ typedef struct {
     int64_t kernel_launches;  /* kernels this library launched in the setup  */
     double bucket_flops[4];   /* algorithmic (folded) flops per bucket kernel */
     int64_t reused_columns;   /* columns that took an identical column's solution (-cs/-ch) */
+    int64_t factor_reuse_columns; /* columns that converged from their kept factor */
 } mspai_stats;
 
 typedef struct mspai_handle mspai_handle;

@@ -37,7 +37,7 @@ class mspai_params(ctypes.Structure):
                 ("probing", ctypes.c_int32), ("prec", ctypes.c_int32), ("refine", ctypes.c_int32),
                 ("batched", ctypes.c_int32), ("verbose", ctypes.c_int32),
                 ("col_begin", ctypes.c_int32), ("col_end", ctypes.c_int32),
-                ("keep_factors", ctypes.c_int32)]
+                ("keep_factors", ctypes.c_int32), ("reuse_factors", ctypes.c_int32)]
 
 
 class mspai_stats(ctypes.Structure):
@@ -48,7 +48,7 @@ class mspai_stats(ctypes.Structure):
                 ("gather_bytes", ctypes.c_double), ("setup_ms", ctypes.c_double),
                 ("kernel_ms", ctypes.c_double * 4), ("kernel_launches", ctypes.c_int64),
                 ("bucket_flops", ctypes.c_double * 4),
-                ("reused_columns", ctypes.c_int64)]
+                ("reused_columns", ctypes.c_int64), ("factor_reuse_columns", ctypes.c_int64)]
 
 
 class mspai_matrix(ctypes.Structure):

@@ -44,12 +44,13 @@ class Options:
     target: int = 1
     probing: int = 0
     prec: str = "mixed"        # "fp64" or "mixed"
-    refine: int = 2
+    refine: int = 4
     batched: bool = True
     verbose: int = 0
     col_begin: int = 0         # solve only columns [col_begin, col_end) (0, 0: all)
     col_end: int = 0
-    keep_factors: bool = False  # keep every column's R for the adjoint's gbar term
+    keep_factors: bool = False  # keep every column's R (adjoint's gbar term, re-setups)
+    reuse_factors: int = 0      # > 0: re-setup from the kept factors, at most this many steps
 
     def to_c(self) -> mspai_params:
         p = mspai_params()
@@ -58,6 +59,7 @@ class Options:
                   "rho", "bs", "target", "probing", "refine", "verbose", "col_begin", "col_end"):
             setattr(p, f, getattr(self, f))
         p.keep_factors = 1 if self.keep_factors else 0
+        p.reuse_factors = int(self.reuse_factors)
         p.prec = _lib.PREC_FP64 if self.prec == "fp64" else _lib.PREC_MIXED
         p.batched = 1 if self.batched else 0
         return p
@@ -266,6 +268,7 @@ class Handle:
             "setup_ms": s.setup_ms, "kernel_ms": list(s.kernel_ms),
             "kernel_launches": s.kernel_launches, "bucket_flops": list(s.bucket_flops),
             "reused_columns": s.reused_columns,
+            "factor_reuse_columns": s.factor_reuse_columns,
         }
 
     def adjoint(self, C: MatrixLike, B: Optional[MatrixLike] = None,

@@ -1095,6 +1095,169 @@ __device__ bool fixed_solve_column(const CtaGroup<NT>& g, FixShared<T>& fs, cons
     g.sync();
     PHASE_MARK(1);
 
+    // FP64 residual r = b - C(I, J) x on the shared rows, its squared norm
+    // with the singleton rows' part from d0 and the target entries kept
+    // apart; with grad, C^T r into gv (in T)
+    auto residual = [&](bool grad, T* gv) -> double {
+        double part = 0.0;
+        for (int d = tid; d < S; d += NT) {
+            const int s = sof[d];
+            double v = bd[d];
+            for (int t = gstart[s]; t < gstart[s + 1]; t++) {
+                const int q = rq[t];
+                v -= csh_v[q] * x[csh_jj[q]];
+            }
+            rd[d] = v;
+            part += v * v;
+        }
+        for (int jj = tid; jj < n; jj += NT)
+            part += x[jj] * x[jj] * d0sq[jj];
+        if (tid == 0)
+            for (int s = 0; s < nspec; s++) {
+                const double r = fs.spec_b[s] - fs.spec_v[s] * x[fs.spec_jj[s]];
+                part += r * r;
+            }
+        const double r2 = g.sum(part);  // includes a barrier: rd is complete
+        if (grad) {
+            for (int jj = tid; jj < n; jj += NT) {
+                double acc = -x[jj] * d0sq[jj];
+                for (int q = cstart[jj]; q < cstart[jj + 1]; q++)
+                    acc += csh_v[q] * rd[csh_d[q]];
+                for (int s = 0; s < nspec; s++)
+                    if (fs.spec_jj[s] == jj)
+                        acc += fs.spec_v[s] * (fs.spec_b[s] - fs.spec_v[s] * x[jj]);
+                gv[jj] = static_cast<T>(acc);
+            }
+            g.sync();
+        }
+        return r2;
+    };
+    // Refinement x += R^-1 R^-T C^T (b - C x), gv holding C^T r on entry, at
+    // most max_steps steps; r2 is updated.  Returns true when the last
+    // correction fell below 2^-44 of the solution (converged); stops early
+    // when the corrections no longer contract.
+    int ref_steps = 0;  // refinement steps taken
+    auto refine = [&](const T* R, const T* Dinv, T* gv, int max_steps, double& r2) -> bool {
+        double d2_prev = 0.0;
+        for (int it = 0; it < max_steps; it++) {
+            ref_steps++;
+            if (Dinv) {
+                fix_forward_inv<T, NT>(g, R, Dinv, n, gv);
+                fix_back_inv<T, NT>(g, R, Dinv, n, gv);
+            }
+            else {
+                fix_forward_substitute<T, NT>(g, R, n, gv);
+                fix_back_substitute<T, NT>(g, R, n, gv);
+            }
+            double d2 = 0.0, x2 = 0.0;
+            for (int i = tid; i < n; i += NT) {
+                const double dl = static_cast<double>(gv[i]);
+                const double x1 = x[i] + dl;
+                d2 += dl * dl;
+                x2 += x1 * x1;
+                x[i] = x1;
+            }
+            d2 = g.sum(d2);
+            x2 = g.sum(x2);
+            // converged (correction below 2^-44 of the solution), or no
+            // longer contracting (R too far from this column's matrix)
+            const bool conv = d2 <= 0x1p-88 * x2;
+            const bool last = conv || (it + 1 == max_steps) || (it > 0 && d2 > 0.25 * d2_prev);
+            d2_prev = d2;
+            r2 = residual(!last, gv);
+            if (last)
+                return conv;
+        }
+        return false;
+    };
+    // outputs (M has P's pattern: values only); fwork: the folded flops done
+    auto finish = [&](double r2, int sing, double fwork) {
+        const double res = sqrt(r2);
+        int nonfinite = 0;
+        for (int t = tid; t < n; t += NT) {
+            const double v = x[t];
+            if (!isfinite(v))
+                nonfinite = 1;
+            out.oval[p0 + t] = v;
+        }
+        nonfinite = g.sum(nonfinite);
+        if (tid == 0) {
+            const double dn = n, dm = m;
+            double* wk = out.work + 3 * static_cast<size_t>(col);
+            wk[0] += fwork;
+            wk[1] += 2.0 * dm * dn * dn - (2.0 / 3.0) * dn * dn * dn + 4.0 * dm * dn + 2.0 * dm * dn;
+            wk[2] += 12.0 * E + 16.0 * dn + 8.0 * dm;
+            out.olen[col] = n;
+            out.res[col] = res;
+            out.steps[col] = 1;
+            out.status[col] = sing ? 1 : ((nonfinite || !isfinite(res)) ? 2 : 0);
+        }
+        g.sync();
+    };
+
+    // ---- re-setup from the kept factor: the previous solution and R, FP64
+    // refinement against the new values; not converged -> factored below
+    if (out.reuse_steps > 0 && out.rstore) {
+        FixArena b2 = a;
+        b2.hi = arena_cap;  // the transient arrays are dead
+        const int r_el = fix_rs(n, n);
+        T* gv = b2.low<T>(n);
+        T* Rr = nullptr;
+        if (b2.ok()) {
+            FixArena b3 = b2;
+            T* rr = b3.low<T>(r_el);
+            if (b3.ok()) {
+                Rr = rr;
+                b2 = b3;
+            }
+            else if (rglob != nullptr && rglob_elems >= r_el) {
+                Rr = rglob;
+            }
+        }
+        if (Rr != nullptr) {
+            const T* src = static_cast<const T*>(out.rstore) + out.roff[col];
+            for (int t = tid; t < n * (n + 1) / 2; t += NT) {
+                int j = static_cast<int>((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
+                while (j * (j + 1) / 2 > t)
+                    j--;
+                while ((j + 1) * (j + 2) / 2 <= t)
+                    j++;
+                const int i = t - j * (j + 1) / 2;
+                Rr[fix_rs(i, n) + (j - i)] = src[t];
+            }
+            for (int t = tid; t < n; t += NT)
+                x[t] = out.oval[p0 + t];
+            g.sync();
+            int zero = 0;
+            for (int i = tid; i < n; i += NT)
+                if (Rr[fix_rs(i, n)] == T(0))
+                    zero = 1;
+            zero = g.sum(zero);
+            if (!zero) {
+                T* Dr = nullptr;
+                const int nblk = (n + kFixPanel - 1) / kFixPanel;
+                FixArena b4 = b2;
+                T* dd = b4.low<T>(kFixPanel * kFixPanel * nblk);
+                const bool r_smem = reinterpret_cast<char*>(Rr) >= arena_base &&
+                                    reinterpret_cast<char*>(Rr) < arena_base + arena_cap;
+                if (r_smem && b4.ok()) {
+                    Dr = dd;
+                    fix_invert_diag<T, NT>(Rr, n, Dr);
+                    g.sync();
+                }
+                double r2 = residual(true, gv);
+                if (refine(Rr, Dr, gv, out.reuse_steps, r2)) {
+                    // per step: two triangular solves, the residual and C^T r
+                    finish(r2, 0, (ref_steps + 1.0) * (2.0 * n * n + 4.0 * SEn + 3.0 * n));
+                    if (tid == 0)
+                        atomicAdd(out.reuse_count, 1);
+                    return true;
+                }
+            }
+            g.sync();  // every thread is done with the kept factor's arrays
+        }
+    }
+
     // ---- skyline of the shared rows, diagonal rows H, [R, Q^T b]
     const int ldw = (n + 1 + 3) & ~3;
     for (int d = tid; d < S; d += NT)
@@ -1245,84 +1408,14 @@ __device__ bool fixed_solve_column(const CtaGroup<NT>& g, FixShared<T>& fs, cons
     PHASE_MARK(6);
 
     // ---- FP64 residual (and refinement in mixed mode)
-    auto residual = [&](bool grad) -> double {
-        double part = 0.0;
-        for (int d = tid; d < S; d += NT) {
-            const int s = sof[d];
-            double v = bd[d];
-            for (int t = gstart[s]; t < gstart[s + 1]; t++) {
-                const int q = rq[t];
-                v -= csh_v[q] * x[csh_jj[q]];
-            }
-            rd[d] = v;
-            part += v * v;
-        }
-        for (int jj = tid; jj < n; jj += NT)
-            part += x[jj] * x[jj] * d0sq[jj];
-        if (tid == 0)
-            for (int s = 0; s < nspec; s++) {
-                const double r = fs.spec_b[s] - fs.spec_v[s] * x[fs.spec_jj[s]];
-                part += r * r;
-            }
-        const double r2 = g.sum(part);  // includes a barrier: rd is complete
-        if (grad) {
-            for (int jj = tid; jj < n; jj += NT) {
-                double acc = -x[jj] * d0sq[jj];
-                for (int q = cstart[jj]; q < cstart[jj + 1]; q++)
-                    acc += csh_v[q] * rd[csh_d[q]];
-                for (int s = 0; s < nspec; s++)
-                    if (fs.spec_jj[s] == jj)
-                        acc += fs.spec_v[s] * (fs.spec_b[s] - fs.spec_v[s] * x[jj]);
-                yv[jj] = static_cast<T>(acc);
-            }
-            g.sync();
-        }
-        return r2;
-    };
-    double r2 = residual(!sing && pb.refine > 0);
-    if (!sing) {
-        for (int it = 0; it < pb.refine; it++) {
-            if (Dinv) {
-                fix_forward_inv<T, NT>(g, Rst, Dinv, n, yv);
-                fix_back_inv<T, NT>(g, Rst, Dinv, n, yv);
-            }
-            else {
-                fix_forward_substitute<T, NT>(g, Rst, n, yv);
-                fix_back_substitute<T, NT>(g, Rst, n, yv);
-            }
-            double d2 = 0.0, x2 = 0.0;
-            for (int i = tid; i < n; i += NT) {
-                const double dl = static_cast<double>(yv[i]);
-                const double x1 = x[i] + dl;
-                d2 += dl * dl;
-                x2 += x1 * x1;
-                x[i] = x1;
-            }
-            d2 = g.sum(d2);
-            x2 = g.sum(x2);
-            const bool last = (it + 1 == pb.refine) || d2 <= 0x1p-88 * x2;
-            r2 = residual(!last);
-            if (last)
-                break;
-        }
-    }
-    const double res = sqrt(r2);
+    double r2 = residual(!sing && pb.refine > 0, yv);
+    if (!sing)
+        refine(Rst, Dinv, yv, pb.refine, r2);
     PHASE_MARK(7);
-
-    // ---- outputs (M has P's pattern: values only)
-    int nonfinite = 0;
-    for (int t = tid; t < n; t += NT) {
-        const double v = x[t];
-        if (!isfinite(v))
-            nonfinite = 1;
-        out.oval[p0 + t] = v;
-    }
-    nonfinite = g.sum(nonfinite);
-    if (tid == 0) {
-        // algorithmic work: the skyline QR (panel factorization and compact-WY
-        // update), Q^T b, the solve and the FP64 residual; the dense-equivalent
-        // count of dgeqrf on C(I, J); the gather bytes
-        double f = 0.0;
+    // algorithmic work: the skyline QR (panel factorization and compact-WY
+    // update), Q^T b, the solve and the FP64 residual
+    double fwork = 0.0;
+    {
         int ap = 0;
         for (int p = 0; p < npan; p++) {
             const int c0 = p * kFixPanel;
@@ -1330,19 +1423,11 @@ __device__ bool fixed_solve_column(const CtaGroup<NT>& g, FixShared<T>& fs, cons
             while (ap < S && c0row[ap] <= c0)
                 ap++;
             const double mp = nb + ap, nc = n + 1 - c0 - nb;
-            f += 2.0 * mp * nb * nb - (2.0 / 3.0) * nb * nb * nb + 4.0 * mp * nb * nc;
+            fwork += 2.0 * mp * nb * nb - (2.0 / 3.0) * nb * nb * nb + 4.0 * mp * nb * nc;
         }
-        const double dn = n, dm = m;
-        double* wk = out.work + 3 * static_cast<size_t>(col);
-        wk[0] += f + dn * dn + 2.0 * E;
-        wk[1] += 2.0 * dm * dn * dn - (2.0 / 3.0) * dn * dn * dn + 4.0 * dm * dn + 2.0 * dm * dn;
-        wk[2] += 12.0 * E + 16.0 * dn + 8.0 * dm;
-        out.olen[col] = n;
-        out.res[col] = res;
-        out.steps[col] = 1;
-        out.status[col] = sing ? 1 : ((nonfinite || !isfinite(res)) ? 2 : 0);
+        fwork += static_cast<double>(n) * n + 2.0 * E;
     }
-    g.sync();
+    finish(r2, sing, fwork);
     return true;
 }
 

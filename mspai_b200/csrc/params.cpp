@@ -31,12 +31,13 @@ extern "C" void mspai_default_params(mspai_params* p)
     p->target = 1;
     p->probing = 0;
     p->prec = MSPAI_PREC_MIXED;
-    p->refine = 2;
+    p->refine = 4;
     p->batched = 1;
     p->verbose = 0;
     p->col_begin = 0;
     p->col_end = 0;
     p->keep_factors = 0;
+    p->reuse_factors = 0;
 }
 
 static int fail(char* msg, int len, const char* text)
@@ -147,6 +148,11 @@ extern "C" int mspai_validate_params(const mspai_params* p, char* msg, int32_t l
     }
     if (p->prec != MSPAI_PREC_FP64 && p->prec != MSPAI_PREC_MIXED) {
         std::snprintf(buf, sizeof(buf), "Illegal precision: %d", p->prec);
+        return fail(msg, len, buf);
+    }
+    if (p->reuse_factors < 0 || p->reuse_factors > 64) {
+        std::snprintf(buf, sizeof(buf), "Illegal number of re-setup refinement steps: %d",
+                      p->reuse_factors);
         return fail(msg, len, buf);
     }
     if (p->refine < 0 || p->refine > 16) {

@@ -32,6 +32,10 @@ constexpr int kLists = 4;      // work lists: buckets + the overflow lists
 // Arena of the fixed-pattern solver's second launch (one CTA per SM): the
 // largest dynamic shared memory a CTA may have beside the solver's static part.
 constexpr int kFixedArenaLarge = 212 * 1024;
+// Mixed precision solves a bucket whose largest |J_k| (after the pattern
+// updates) is at most this in FP64 directly: the FP32 QR saves nothing on such
+// sizes, and the refinement would add two passes over the column's entries.
+constexpr int kMixedFp64MaxN = 32;
 
 // A device buffer that grows on demand.
 struct DevBuf {
@@ -92,8 +96,10 @@ struct mspai_handle {
     DevBuf rkeys, rslot_rep, rslot_of, rrep;  // reuse table
     DevBuf rglob;  // per-CTA areas for R of the fixed-pattern solver
     DevBuf rstore, roff;  // R of every column (keep_factors), packed by columns
+    DevBuf rhash;         // structure digest of C, P, B (device accumulator)
     bool r_valid = false;
     int r_elem = 8;
+    unsigned long long r_hash = 0;  // digest of the setup whose R is kept
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t evb[2 * kKernels] = {};
     // result description
@@ -533,7 +539,31 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     out.steps = h->steps.as<int32_t>();
     out.status = h->status.as<int32_t>();
     out.work = h->work.as<double>();
-    // ---- the columns' triangular factors for the adjoint (fixed scalar patterns)
+    // ---- the columns' triangular factors for the adjoint and for re-setups
+    // (fixed scalar patterns)
+    bool reuse_now = false;
+    unsigned long long shash = 0;
+    if (prm->keep_factors && !compact) {
+        // digest of the structures of C, P and B: a re-setup from the kept
+        // factors needs the structure of the setup that kept them
+        CUDA_TRY(h, h->rhash.ensure(sizeof(unsigned long long)));
+        auto* acc = h->rhash.as<unsigned long long>();
+        CUDA_TRY(h, cudaMemsetAsync(acc, 0, sizeof(unsigned long long), st));
+        h->launches += pb.bptr ? 3 : 2;
+        CUDA_TRY(h, mspai::launch_structure_hash(pb.cptr, pb.cidx, n, C->nnz,
+                                                 0x436f6c756d6e73ull, acc, st));
+        CUDA_TRY(h, mspai::launch_structure_hash(pb.pptr, pb.pidx, nprob, P->nnz,
+                                                 0x5061747465726eull, acc, st));
+        if (pb.bptr)
+            CUDA_TRY(h, mspai::launch_structure_hash(pb.bptr, pb.bidx, n, B->nnz,
+                                                     0x546172676574ull, acc, st));
+        CUDA_TRY(h, cudaMemcpyAsync(&shash, acc, sizeof(shash), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(h, cudaStreamSynchronize(st));
+        shash ^= (static_cast<unsigned long long>(C->nrows) << 32) ^
+                 static_cast<unsigned long long>(elem);
+        reuse_now = prm->reuse_factors > 0 && h->r_valid && h->r_hash == shash &&
+                    h->r_elem == elem && !partial && prm->batched;
+    }
     h->r_valid = false;
     if (prm->keep_factors && !compact) {
         CUDA_TRY(h, h->cap_len.ensure(sizeof(int32_t) * std::max(n, 1)));
@@ -550,6 +580,12 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
         out.rstore = h->rstore.p;
         out.roff = h->roff.as<int64_t>();
         h->r_elem = elem;
+        if (reuse_now) {
+            // M's previous values are still in oval (same structure, no range)
+            out.reuse_steps = prm->reuse_factors;
+            out.reuse_count = h->counters.as<int32_t>() + 40;
+            CUDA_TRY(h, cudaMemsetAsync(out.reuse_count, 0, sizeof(int32_t), st));
+        }
     }
 
     // ---- plan and bucket
@@ -618,18 +654,18 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     h->used_fixed = use_fixed;
     // general CTA solver over `count` listed columns with the given caps
     auto run_cta = [&](int b, const Caps& cap, int32_t* list, int count, int32_t* counter,
-                       size_t wsm_budget) -> int {
+                       size_t wsm_budget, int elem_b, const Problem& pbb) -> int {
         int grid = 0;
-        size_t wsm = std::min<size_t>(mspai::w_bytes(cap, elem), wsm_budget);
+        size_t wsm = std::min<size_t>(mspai::w_bytes(cap, elem_b), wsm_budget);
         if (!prm->batched)
             wsm = 0;  // the plain path keeps W in global memory, unblocked
-        const size_t need = mspai::cta_scratch_needed(elem, cap, count, wsm);
+        const size_t need = mspai::cta_scratch_needed(elem_b, cap, count, wsm);
         CUDA_TRY(h, h->scratch.ensure(need));
         if (adaptive)  // the candidate bit vectors of the slots start cleared
             CUDA_TRY(h, cudaMemsetAsync(h->scratch.p, 0, need, st));
         CUDA_TRY(h, cudaMemsetAsync(counter, 0, sizeof(int32_t), st));
         h->launches++;
-        CUDA_TRY(h, mspai::launch_cta_solve(elem, wsm, prm->batched != 0, pb, cap, out, list,
+        CUDA_TRY(h, mspai::launch_cta_solve(elem_b, wsm, prm->batched != 0, pbb, cap, out, list,
                                             count, counter, h->scratch.as<char>(),
                                             h->scratch.bytes, st, &grid));
         (void)b;
@@ -663,14 +699,21 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
         int32_t* counter = dcnt + 12 + b;
         CUDA_TRY(h, cudaMemsetAsync(counter, 0, sizeof(int32_t), st));
         int grid = 0;
+        // small problems in mixed mode: FP64 without refinement (not when R
+        // is kept: its store has one element type)
+        const bool fp64_bucket = mixed && !out.rstore && cap.nmax <= kMixedFp64MaxN;
+        const int elem_b = fp64_bucket ? 8 : elem;
+        Problem pbb = pb;
+        if (fp64_bucket)
+            pbb.refine = 0;
         bool use_warp = (b == 0);
         if (use_warp &&
-            mspai::warp_slot_bytes(cap, elem) * (mspai::kWarpKernelThreads / 32) > 200 * 1024)
+            mspai::warp_slot_bytes(cap, elem_b) * (mspai::kWarpKernelThreads / 32) > 200 * 1024)
             use_warp = false;
         if (use_warp) {
             CUDA_TRY(h, cudaEventRecord(h->evb[0], st));
             h->launches++;
-            CUDA_TRY(h, mspai::launch_warp_solve(elem, pb, cap, out, list, count, counter, st,
+            CUDA_TRY(h, mspai::launch_warp_solve(elem_b, pbb, cap, out, list, count, counter, st,
                                                  &grid));
             CUDA_TRY(h, cudaEventRecord(h->evb[1], st));
             timed[0] = true;
@@ -711,7 +754,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
             h->stats.bucket_columns[3] = ho[1];
             if (ho[1] > 0) {
                 CUDA_TRY(h, cudaEventRecord(h->evb[6], st));
-                const int rc2 = run_cta(3, cap, ovf_b, ho[1], dcnt + 15, 48 * 1024);
+                const int rc2 = run_cta(3, cap, ovf_b, ho[1], dcnt + 15, 48 * 1024, elem, pb);
                 if (rc2 != MSPAI_OK)
                     return rc2;
                 CUDA_TRY(h, cudaEventRecord(h->evb[7], st));
@@ -720,7 +763,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
         }
         else {
             CUDA_TRY(h, cudaEventRecord(h->evb[2 * b], st));
-            const int rc2 = run_cta(b, cap, list, count, counter, h->smem_budget);
+            const int rc2 = run_cta(b, cap, list, count, counter, h->smem_budget, elem_b, pbb);
             if (rc2 != MSPAI_OK)
                 return rc2;
             CUDA_TRY(h, cudaEventRecord(h->evb[2 * b + 1], st));
@@ -801,6 +844,13 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     h->last_params = *prm;
     h->have_result = true;
     h->r_valid = out.rstore != nullptr;
+    h->r_hash = shash;
+    h->stats.factor_reuse_columns = 0;
+    if (out.reuse_count) {
+        int32_t nr = 0;
+        CUDA_TRY(h, cudaMemcpy(&nr, out.reuse_count, sizeof(int32_t), cudaMemcpyDeviceToHost));
+        h->stats.factor_reuse_columns = nr;
+    }
     return MSPAI_OK;
 }
 
@@ -845,6 +895,7 @@ int mspai_tune(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, con
     }
     h->smem_budget = static_cast<size_t>(best) * 1024;
     h->have_result = false;  // the sample runs are not a result
+    h->r_valid = false;
     if (smem_kb_out)
         *smem_kb_out = best;
     return MSPAI_OK;

@@ -212,6 +212,50 @@ __global__ void finish_ptr_kernel(int64_t* __restrict__ ptr, int n, const int32_
 }
 
 // entries of a packed triangle of |P(:, k)|: n_k (n_k + 1) / 2
+// Order-independent 64-bit digest of a CSC structure: the wrapping sum of a
+// mix of (position, value) over the column pointers and the row indices, so
+// that the result does not depend on the launch shape or the order of the
+// atomic adds.
+__device__ __forceinline__ unsigned long long struct_mix(unsigned long long v)
+{
+    // SplitMix64 finaliser
+    v += 0x9e3779b97f4a7c15ull;
+    v = (v ^ (v >> 30)) * 0xbf58476d1ce4e5b9ull;
+    v = (v ^ (v >> 27)) * 0x94d049bb133111ebull;
+    return v ^ (v >> 31);
+}
+
+__global__ void structure_hash_kernel(const int64_t* __restrict__ ptr,
+                                      const int32_t* __restrict__ idx, int ncols, int64_t nnz,
+                                      unsigned long long salt, unsigned long long* acc)
+{
+    unsigned long long part = 0;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i <= ncols;
+         i += stride)
+        part += struct_mix(salt ^ (static_cast<unsigned long long>(i) << 1) ^
+                           (static_cast<unsigned long long>(ptr[i]) * 0x100000001b3ull));
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < nnz;
+         i += stride)
+        part += struct_mix(~salt ^ (static_cast<unsigned long long>(i) << 1) ^
+                           (static_cast<unsigned long long>(static_cast<uint32_t>(idx[i])) << 33));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        part += __shfl_xor_sync(0xffffffffu, part, o);
+    if ((threadIdx.x & 31) == 0)
+        atomicAdd(acc, part);
+}
+
+cudaError_t launch_structure_hash(const int64_t* ptr, const int32_t* idx, int ncols, int64_t nnz,
+                                  unsigned long long salt, unsigned long long* acc,
+                                  cudaStream_t st)
+{
+    const int blocks = std::max(1, std::min<int>(num_sms() * 8,
+                                                 static_cast<int>((nnz + ncols + 255) / 256)));
+    structure_hash_kernel<<<blocks, 256, 0, st>>>(ptr, idx, ncols, nnz, salt, acc);
+    return cudaGetLastError();
+}
+
 __global__ void tri_len_kernel(const int64_t* __restrict__ pptr, int n, int32_t* __restrict__ len)
 {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {

@@ -85,6 +85,11 @@ cudaError_t launch_fixed_solve(int elem_bytes, int arena_bytes, const Problem& p
 cudaError_t launch_scan_lengths(const int32_t* len, int n, int64_t* ptr, int64_t* tmp,
                                 cudaStream_t st);
 // len[k] = |P(:, k)| (|P(:, k)| + 1) / 2 (packed triangles of the kept R)
+// Adds an order-independent 64-bit digest of a CSC structure (pointers and
+// row indices) to *acc.
+cudaError_t launch_structure_hash(const int64_t* ptr, const int32_t* idx, int ncols, int64_t nnz,
+                                  unsigned long long salt, unsigned long long* acc,
+                                  cudaStream_t st);
 cudaError_t launch_tri_len(const int64_t* pptr, int n, int32_t* len, cudaStream_t st);
 cudaError_t launch_capacity_len(const int64_t* pptr, int n, int bs, int grow, int32_t* len,
                                 cudaStream_t st);

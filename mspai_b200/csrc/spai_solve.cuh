@@ -72,6 +72,12 @@ struct Output {
     // R(i, j) at rstore + roff[k] + j (j + 1) / 2 + i, in the solve's precision
     void* rstore;
     const int64_t* roff;
+    // re-setup from the kept factors (fixed-pattern solver): start from M's
+    // previous values in oval and the R in rstore, at most reuse_steps FP64
+    // refinement steps against the new values; a column that does not
+    // converge is factored again.  reuse_count counts the columns that converged.
+    int reuse_steps;
+    int32_t* reuse_count;
 };
 
 // Capacities of one problem slot.
@@ -808,8 +814,10 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
         // staged in the shared area); W in shared memory: the dense blocked QR
         const bool structured = !qru && !w_smem && (G::kWarps > 1) && s.bsc != nullptr &&
                                 s.Wfast && (kPanel + S) * kPanel <= s.wfast_elems;
-        const bool blocked =
-            !qru && (G::kWarps > 1) && s.bsc != nullptr && (w_smem || structured);
+        // (up to two panels the unblocked QR, a warp per trailing column, has
+        // the shorter dependency chain)
+        const bool blocked = !qru && (G::kWarps > 1) && s.bsc != nullptr &&
+                             (structured || (w_smem && n > 2 * kPanel));
         T* W = w_smem ? s.Wfast : s.W;
         const int ld = qru ? cap.emax : (structured ? kPanel + S : mw);
         const int r0 = structured ? kPanel : 0;  // first shared row in W
@@ -1032,6 +1040,7 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
             r2 = resid_grad();
             if (!sing && pb.refine > 0) {
                 group_diag_reciprocals<T>(g, rq, n, s.rinv);
+                double d2_prev = 0.0;
                 for (int it = 0; it < pb.refine; it++) {
                     for (int c = 0; c < nrhs; c++)
                         group_normal_correction_rl<T>(g, rq, n, s.rinv,
@@ -1046,8 +1055,10 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
                     d2 = g.sum(d2);
                     x2 = g.sum(x2);
                     r2 = resid_grad();
-                    if (d2 <= 0x1p-88 * x2)
+                    // converged, or no longer contracting
+                    if (d2 <= 0x1p-88 * x2 || (it > 0 && d2 > 0.25 * d2_prev))
                         break;
+                    d2_prev = d2;
                 }
             }
         }
@@ -1055,6 +1066,7 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
             r2 = group_residual(g, pb, col, s.keys, s.I, s.rstart, s.ejj, s.ev, s.x, s.r, m, n,
                                 nrhs);
         if (!sing && !fixed) {
+            double d2_prev = 0.0;
             for (int it = 0; it < pb.refine; it++) {
                 g.sync();
                 for (int t = g.warp(); t < n * nrhs; t += G::kWarps) {
@@ -1100,9 +1112,11 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
                 r2 = group_residual(g, pb, col, s.keys, s.I, s.rstart, s.ejj, s.ev, s.x, s.r, m,
                                     n, nrhs);
                 // converged: ||delta|| <= 2^-44 ||x||; the next correction would be
-                // smaller again by about kappa^2 * u_fp32, far below FP64 rounding
-                if (d2 <= 0x1p-88 * x2)
+                // smaller again by about kappa^2 * u_fp32, far below FP64 rounding.
+                // No longer contracting: FP32 R is too far from this column's matrix
+                if (d2 <= 0x1p-88 * x2 || (it > 0 && d2 > 0.25 * d2_prev))
                     break;
+                d2_prev = d2;
             }
         }
         res = sqrt(r2);
