@@ -76,6 +76,7 @@ struct FixShared {
     T tot2[kFixPanel];              // reduced sums of one step (warp panel)
     T tau[kFixPanel];
     T red[2][16][kFixPanel];        // per-warp column sums of one panel step (two buffers)
+    T pkrow[2][kFixPanel];          // row k of the panel at step k (CTA panel, two buffers)
     int tg_row[kFixMaxSpecial];     // target column: rows and values
     double tg_val[kFixMaxSpecial];
     int nspec;
@@ -358,6 +359,7 @@ __device__ void fix_panel_qr_rows(FixShared<T>& fs, T* tb, const int32_t* prow, 
 {
     constexpr int NW = NT / 32;
     constexpr int G = 2 * NW;
+    static_assert(G >= kFixPanel, "row k of the panel is the first row of group k");
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int c = lane & 15;
@@ -388,6 +390,11 @@ __device__ void fix_panel_qr_rows(FixShared<T>& fs, T* tb, const int32_t* prow, 
         T(*red)[kFixPanel] = fs.red[k & 1];
         if (lane < kFixPanel)
             red[warp][lane] = acc;
+        // row k as it stands before step k, published with the sums: its
+        // owner (group k, rows k, k + G, ...; k < 16 <= G) updates it in this
+        // step while other warps may still be reading it
+        if (grp == k)
+            fs.pkrow[k & 1][c] = tb[ro[0] + c];
         __syncthreads();
         FIX_SUB(10);
         T tot = T(0), x2 = T(0);
@@ -396,9 +403,8 @@ __device__ void fix_panel_qr_rows(FixShared<T>& fs, T* tb, const int32_t* prow, 
             tot += red[w][c];
             x2 += red[w][k];
         }
-        const T* pk = tb + prow[k];
-        const T alpha = pk[k];
-        const T rkc = pk[c];
+        const T alpha = fs.pkrow[k & 1][k];
+        const T rkc = fs.pkrow[k & 1][c];
         T tau = T(0), scale = T(0), beta = alpha;
         if (x2 != T(0)) {
             beta = -copysign(tsqrt<T>(alpha * alpha + x2), alpha);
