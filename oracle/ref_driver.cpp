@@ -36,6 +36,13 @@
  *   -repeat r   with a column subset: run the column loop r times after one
  *               read of the inputs (each pass recomputes the same columns)
  *   -time f     write {"setup_s":…, "columns":…, "rep_s": [...]} as JSON to f
+ *   -gpu fp64|mixed   (ref_driver_gpu only, built with MSPAI_GPU_SHIM) run the
+ *               library's drop-in mspai_b200_shim::Spai_GPU_Algorithm
+ *               (include/mspai_b200_reference_shim.hpp) in place of
+ *               alg->SPAI_Algorithm, as a maintainer would in
+ *               PC_MSPAI::bspai, and write M with the reference's own
+ *               Write_Matrix_To_File: the stock and the drop-in runs of one
+ *               command line give files that the tests compare
  * With a subset, only the computed columns are written (scalar columns; a
  * block column as its bs scalar columns, through the reference's
  * Matrix::Scalar_Matrix).
@@ -46,6 +53,10 @@
 #include "Read_mm_Matrix.h"
 #include "Spai.h"
 #include "Switch_Algorithm.h"
+
+#ifdef MSPAI_GPU_SHIM
+#include "mspai_b200_reference_shim.hpp"
+#endif
 
 #include <chrono>
 #include <cstdio>
@@ -75,6 +86,7 @@ struct Options {
     const char* col_file = nullptr;
     int repeat = 1;
     const char* time_file = nullptr;
+    const char* gpu = nullptr;  // -gpu fp64|mixed: the library's drop-in
 };
 
 void usage()
@@ -137,6 +149,7 @@ Options parse(int argc, char** argv)
             else { o.up = 0; o.up_file = v; }
         }
         else if (k == "-colfile") o.col_file = v;
+        else if (k == "-gpu") o.gpu = v;
         else if (k == "-repeat") o.repeat = std::atoi(v) > 0 ? std::atoi(v) : 1;
         else if (k == "-cols") {
             if (std::sscanf(v, "%ld:%ld", &o.col_lo, &o.col_hi) != 2)
@@ -291,7 +304,25 @@ int main(int argc, char** argv)
 
         std::vector<double> rep_s;
         auto t0 = std::chrono::steady_clock::now();
-        if (!subset) {
+        if (o.gpu) {
+#ifdef MSPAI_GPU_SHIM
+            if (subset || o.bs != 1)
+                throw std::runtime_error("-gpu runs whole scalar setups");
+            mspai_params extra;
+            mspai_default_params(&extra);
+            extra.cs = o.cs;
+            extra.ch = o.ch;
+            extra.qr = o.qr;
+            extra.hs = o.hs;
+            extra.prec = std::strcmp(o.gpu, "fp64") ? MSPAI_PREC_MIXED : MSPAI_PREC_FP64;
+            mspai_b200_shim::Spai_GPU_Algorithm(A_sys, M, B, P, UP, o.ep, o.mn, o.ns,
+                                                hash_param, o.um, o.pk, o.pm, /*count=*/1,
+                                                o.vb, &extra);
+#else
+            throw std::runtime_error("-gpu: this driver was built without the drop-in");
+#endif
+        }
+        else if (!subset) {
             alg->SPAI_Algorithm(A_sys, M, B, P, UP, o.ep, o.mn, o.ns, hash_param, o.um, o.pk,
                                 o.pm, /*count=*/1, o.vb);
         }

@@ -160,3 +160,26 @@ def test_overflow_chain_gives_identical_columns(tmp_path, arena, large):
         ra = np.load(dbase / f"{prec}_res.npy")
         rb = np.load(dsmall / f"{prec}_res.npy")
         assert np.allclose(ra, rb, rtol=1e-9, atol=1e-14)
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_repeated_setups_are_bit_identical(prec):
+    """Two setups of the same 300,000-column problem give bit-identical M
+    (every reduction of the solvers has a fixed order; a race in a panel
+    factorization showed here as differences of 1e-14 in a few dozen columns
+    that the FP64 refinement had smoothed over)."""
+    import torch
+    w = W.ragged(300000, seed=77)
+    h = mb.Handle(0)
+    try:
+        dA = mb.DeviceCSC.from_scipy(w.A)
+        dP = mb.DeviceCSC.from_scipy(w.P, pattern=True)
+        vals = []
+        for _ in range(2):
+            h.setup(dA, dP, options=mb.Options(ns=0, prec=prec))
+            v = torch.empty(w.P.nnz, dtype=torch.float64, device="cuda")
+            h.result_into(None, None, v, device=True)
+            vals.append(v)
+        assert torch.equal(vals[0], vals[1])
+    finally:
+        h.close()
