@@ -533,11 +533,12 @@ def bench_ours(args):
     achieved = st["bucket_flops"][b] / (kms * 1e-3) / 1e12 if kms > 0 else None
     peak32 = mb.measure_fma_peak(local, fp64=False) / 1e3
     traffic = None
-    prof = os.path.join(HERE, "profiles", "ragged_solve_traffic.json")
-    if os.path.exists(prof):
+    prof = os.path.join(HERE, "profiles", "fixed_solve_traffic.json")
+    if b == 1 and os.path.exists(prof):
         try:
-            # DRAM bytes of one captured launch, scaled to this launch by the
-            # columns it solves (traffic grows with the columns processed)
+            # DRAM bytes of one captured launch A of the fixed-pattern solver,
+            # scaled to this launch by the columns it solves (traffic grows
+            # with the columns processed)
             pj = json.load(open(prof))
             traffic = pj["dram_bytes_per_column"] * st["bucket_columns"][b]
         except Exception:

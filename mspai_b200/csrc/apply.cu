@@ -56,7 +56,8 @@ __global__ void gather_rows_kernel(const int64_t* __restrict__ ptr, int ncols,
                 hi = mid - 1;
         }
         tcol[t] = lo;
-        tval[t] = val[e];
+        if (tval)
+            tval[t] = val[e];
     }
 }
 

@@ -92,7 +92,8 @@ cudaError_t launch_fixed_t(int arena_bytes, const Problem& pb, const Output& out
 int fixed_ctas_per_sm(int arena_bytes)
 {
     // two CTAs of 256 threads per SM (128 registers per thread), or one CTA
-    // of 512 threads with the largest arena
+    // of 256 threads with the largest arena (measured faster than 512 threads:
+    // the barriers of the panel steps wait for half as many warps)
     return arena_bytes <= 107 * 1024 ? 2 : 1;
 }
 
@@ -115,7 +116,7 @@ cudaError_t launch_fixed_solve(int elem_bytes, int arena_bytes, const Problem& p
             return launch_fixed_t<float, 256, 2>(arena_bytes, pb, out, list, count_dev, count_host,
                                                  counter, ovf_list, ovf_count, rglob, rglob_elems,
                                                  max_ctas, st, grid_out);
-        return launch_fixed_t<float, 512, 1>(arena_bytes, pb, out, list, count_dev, count_host,
+        return launch_fixed_t<float, 256, 1>(arena_bytes, pb, out, list, count_dev, count_host,
                                              counter, ovf_list, ovf_count, rglob, rglob_elems,
                                              max_ctas, st, grid_out);
     }
@@ -123,7 +124,7 @@ cudaError_t launch_fixed_solve(int elem_bytes, int arena_bytes, const Problem& p
         return launch_fixed_t<double, 256, 2>(arena_bytes, pb, out, list, count_dev, count_host,
                                               counter, ovf_list, ovf_count, rglob, rglob_elems,
                                               max_ctas, st, grid_out);
-    return launch_fixed_t<double, 512, 1>(arena_bytes, pb, out, list, count_dev, count_host,
+    return launch_fixed_t<double, 256, 1>(arena_bytes, pb, out, list, count_dev, count_host,
                                           counter, ovf_list, ovf_count, rglob, rglob_elems,
                                           max_ctas, st, grid_out);
 }

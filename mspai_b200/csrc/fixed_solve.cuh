@@ -25,11 +25,12 @@
 //     panels; a shared row whose first column lies beyond the panel is zero in
 //     the panel and is not touched by its reflectors, so panel p only involves
 //     the panel's 16 diagonal rows and the shared rows that have started.
-//     The panel is factored by one warp with its rows in registers (one
-//     reduction per column for the norm, the dot products with the later
-//     panel columns and V^T V); the later columns are updated with the compact
-//     WY form by the whole CTA, one column per thread, V rows broadcast from
-//     shared memory.
+//     A panel of up to 64 rows is factored by one warp with its rows in
+//     registers (one reduction per column for the norm, the dot products with
+//     the later panel columns and V^T V), a taller one by the CTA (one barrier
+//     per column); the later columns are updated with the compact WY form by
+//     the whole CTA, two threads per column, V rows broadcast from shared
+//     memory.
 //  4. Back substitution and, in mixed mode, FP64 refinement steps
 //     x += R^-1 R^-T C^T (b - C x): the residual and C^T r in FP64 (step 2),
 //     the two triangular solves with the FP32 R.
@@ -488,14 +489,12 @@ template <class T, int NT>
 __device__ bool fix_panel_qr(FixShared<T>& fs, T* tb, const int32_t* prow, int nb, int mp)
 {
     constexpr int G = 2 * (NT / 32);
-    constexpr int kWarpRows = sizeof(T) == 4 ? 128 : 64;  // register tiling of fix_panel_warp
+    // up to 64 rows the warp panel (two rows per lane); taller panels by the
+    // CTA (four rows per lane in one warp measured slower than the CTA panel)
+    constexpr int kWarpRows = 64;
     if (mp <= kWarpRows) {
-        if (threadIdx.x < 32) {
-            if (mp <= 64)
-                fix_panel_warp<T, 2>(fs, tb, prow, nb, mp);
-            else if constexpr (sizeof(T) == 4)
-                fix_panel_warp<T, 4>(fs, tb, prow, nb, mp);
-        }
+        if (threadIdx.x < 32)
+            fix_panel_warp<T, 2>(fs, tb, prow, nb, mp);
         __syncthreads();
     }
     else if (mp <= 16 * G)

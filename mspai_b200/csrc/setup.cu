@@ -451,18 +451,36 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
             CUDA_TRY(h, fetch(rp, C_rows->colptr, C_rows->ncols + 1, C_rows->mem, st));
         }
         else {
-            std::vector<int64_t> cp;
-            std::vector<int32_t> ci;
-            CUDA_TRY(h, fetch(cp, C->colptr, n + 1, C->mem, st));
-            CUDA_TRY(h, fetch(ci, C->rowidx, C->nnz, C->mem, st));
-            mspai_host::csc_row_structure(n, cp.data(), ci.data(), n, rp, rc2);
-            const int64_t* rpp = nullptr;
-            const int32_t* rcp = nullptr;
-            CUDA_TRY(h, stage(h->rptr, rp.data(), rp.size(), MSPAI_MEM_HOST, st, &rpp));
-            CUDA_TRY(h, stage(h->rcol, rc2.data(), rc2.size(), MSPAI_MEM_HOST, st, &rcp));
-            pb.rptr = rpp;
-            pb.rcol = rcp;
-            CUDA_TRY(h, cudaStreamSynchronize(st));  // host vectors go out of scope
+            // the row structure of C on the device: a stable radix sort of the
+            // entries by row keeps each row's columns ascending; rows below n
+            // are a prefix of it (the probing rows come last)
+            const int nr = C->nrows;
+            const int64_t nz = C->nnz;
+            const size_t tb = mspai::rows_build_temp_bytes(nz, nr);
+            CUDA_TRY(h, h->rptr.ensure(sizeof(int64_t) * (static_cast<size_t>(nr) + 1)));
+            CUDA_TRY(h, h->rcol.ensure(sizeof(int32_t) * std::max<int64_t>(nz, 1)));
+            CUDA_TRY(h, h->tkeys.ensure(sizeof(int32_t) * std::max<int64_t>(nz, 1)));
+            CUDA_TRY(h, h->tperm0.ensure(sizeof(int32_t) * std::max<int64_t>(nz, 1)));
+            CUDA_TRY(h, h->tperm1.ensure(sizeof(int32_t) * std::max<int64_t>(nz, 1)));
+            CUDA_TRY(h, h->tcnt.ensure(sizeof(int32_t) * std::max(nr, 1)));
+            CUDA_TRY(h, h->ttemp.ensure(std::max<size_t>(tb, 16)));
+            CUDA_TRY(h, h->scan_tmp.ensure(sizeof(int64_t) * ((nr + 1023) / 1024 + 2)));
+            h->launches += 7;
+            CUDA_TRY(h, mspai::launch_build_rows(
+                            pb.cptr, pb.cidx, nullptr, n, nr, nz, h->rptr.as<int64_t>(),
+                            h->rcol.as<int32_t>(), nullptr, h->tkeys.as<int32_t>(),
+                            h->tperm0.as<int32_t>(), h->tperm1.as<int32_t>(),
+                            h->tcnt.as<int32_t>(), h->scan_tmp.as<int64_t>(), h->ttemp.p,
+                            h->ttemp.bytes, st));
+            pb.rptr = h->rptr.as<int64_t>();
+            pb.rcol = h->rcol.as<int32_t>();
+            CUDA_TRY(h, h->counters.ensure(64 * sizeof(int32_t)));
+            int32_t* mx = h->counters.as<int32_t>() + 17;
+            h->launches++;
+            CUDA_TRY(h, mspai::launch_max_len(pb.rptr, n, mx, st));
+            CUDA_TRY(h, cudaMemcpyAsync(&max_row_nnz, mx, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                        st));
+            CUDA_TRY(h, cudaStreamSynchronize(st));
         }
         for (size_t i = 0; i + 1 < rp.size(); i++)
             max_row_nnz = std::max<int>(max_row_nnz, static_cast<int>(rp[i + 1] - rp[i]));

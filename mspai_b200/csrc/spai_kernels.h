@@ -28,8 +28,9 @@ struct BucketRule {
 };
 
 // Row structure (CSR) of a CSC matrix, in ascending column order within each
-// row (apply.cu): tptr nrows + 1, tcol/tval nnz; keys_out, perm_in, perm_out
-// nnz and cnt nrows are scratch; temp of rows_build_temp_bytes(nnz, nrows).
+// row (apply.cu): tptr nrows + 1, tcol/tval nnz (tval may be null: structure
+// only); keys_out, perm_in, perm_out nnz and cnt nrows are scratch; temp of
+// rows_build_temp_bytes(nnz, nrows).
 size_t rows_build_temp_bytes(int64_t nnz, int nrows);
 cudaError_t launch_build_rows(const int64_t* ptr, const int32_t* idx, const double* val,
                               int ncols, int nrows, int64_t nnz, int64_t* tptr, int32_t* tcol,
