@@ -502,9 +502,10 @@ def bench_ours(args):
     dP = mb.DeviceCSC.from_scipy(w.P, pattern=True)
     torch.cuda.synchronize()
     mixed = mb.Options(ns=0, prec="mixed", batched=True)
-    # the autotuner picks the solver's shared-memory area per CTA on a sample
-    # of columns (outside the timed region)
-    smem_kb = h.tune(dA, dP, options=mixed, sample_cols=min(n, 50000))
+    # the autotuner picks the launch shapes on a sample of 50,000 columns
+    # (outside the timed region; stored per GPU and configuration class)
+    from mspai_b200 import tuner
+    tuned = tuner.autotune(h, dA, dP, mixed, sample_cols=min(n, 50000))
 
     for _ in range(max(args.warmup, 3) if args.warmup >= 0 else 3):
         h.setup(dA, dP, options=mixed)
@@ -554,7 +555,7 @@ def bench_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded, shapes of the "
-        "ragged 1M-column configuration)", "config": dict(workload_config(n), smem_kb_per_cta=smem_kb),
+        "ragged 1M-column configuration)", "config": dict(workload_config(n), tuning=tuned["tuning"], tuning_cached=tuned["cached"]),
         "roofline": roofline, "clocks": clocks,
         "gpu_launches": int(st["kernel_launches"]) * args.steps,
         "stats": {"buckets": st["bucket_columns"], "kernel_ms": st["kernel_ms"],

@@ -186,6 +186,28 @@ int mspai_result_copy(mspai_handle* h, int64_t* colptr, int32_t* rowidx, double*
                       int32_t mem);
 
 /*
+ * Launch-shape knobs of a handle (no reference counterpart: the reference's
+ * column loop has no launch shape).  The autotuner (mspai_tune, and the
+ * persisted sweep of mspai_b200/tuner.py) chooses them; every setup of the
+ * handle uses them.  Results do not depend on them beyond rounding.
+ */
+typedef struct {
+    int32_t smem_kb;              /* shared-memory area per general-solver CTA, 16..220 (48) */
+    int32_t fixed_arena_kb;       /* arena of the fixed-pattern solver's first launch,
+                                     8..107 (two CTAs per SM) (107)                     */
+    int32_t fixed_arena_large_kb; /* arena of its second launch, 8..212 (212)           */
+    int32_t warp_emax;            /* tiny bucket (a warp per column): at most this many
+                                     entries of C(:,J_k), 16..256 (64)                  */
+    int32_t warp_nmax;            /* ... and |J_k| at most this, 4..32 (16)             */
+    int32_t w_smem_kb;            /* general solver: a column whose folded matrix fits
+                                     this goes to the shared-memory bucket, 16..220 (96) */
+} mspai_tuning;
+
+int mspai_get_tuning(mspai_handle* h, mspai_tuning* t);
+/* Checks every field's range; MSPAI_ERR_PARAM and no change when one is out. */
+int mspai_set_tuning(mspai_handle* h, const mspai_tuning* t);
+
+/*
  * Autotuner (the reference has none: its column loop has no launch shape to
  * pick).  Times setups of problem columns [0, sample_cols) of the given
  * problem (20000 when sample_cols <= 0) with each candidate shared-memory

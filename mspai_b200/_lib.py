@@ -51,6 +51,12 @@ class mspai_stats(ctypes.Structure):
                 ("reused_columns", ctypes.c_int64), ("factor_reuse_columns", ctypes.c_int64)]
 
 
+class mspai_tuning(ctypes.Structure):
+    _fields_ = [("smem_kb", ctypes.c_int32), ("fixed_arena_kb", ctypes.c_int32),
+                ("fixed_arena_large_kb", ctypes.c_int32), ("warp_emax", ctypes.c_int32),
+                ("warp_nmax", ctypes.c_int32), ("w_smem_kb", ctypes.c_int32)]
+
+
 class mspai_matrix(ctypes.Structure):
     _fields_ = [("nrows", ctypes.c_int32), ("ncols", ctypes.c_int32), ("nnz", ctypes.c_int64),
                 ("colptr", ctypes.POINTER(ctypes.c_int64)),
@@ -67,7 +73,7 @@ EXPORTED = [
     "mspai_matrix_view", "mspai_matrix_free", "mspai_mm_read", "mspai_mm_write",
     "mspai_probing_assemble", "mspai_pattern_generate", "mspai_row_structure",
     "mspai_measure_fma_peak", "mspai_setup_fixed_noalloc", "mspai_block_pattern_generate",
-    "mspai_pattern_power2",
+    "mspai_pattern_power2", "mspai_get_tuning", "mspai_set_tuning",
 ]
 
 _lib = None
@@ -100,6 +106,10 @@ def load() -> ctypes.CDLL:
                                P(mspai_csc), P(mspai_params), ctypes.c_int32,
                                P(ctypes.c_int32)]
     lib.mspai_tune.restype = I
+    lib.mspai_get_tuning.argtypes = [V, P(mspai_tuning)]
+    lib.mspai_get_tuning.restype = I
+    lib.mspai_set_tuning.argtypes = [V, P(mspai_tuning)]
+    lib.mspai_set_tuning.restype = I
     lib.mspai_apply.argtypes = [V, V, V, ctypes.c_int32]
     lib.mspai_apply.restype = I
     lib.mspai_column_info.argtypes = [V, V, V, V]

@@ -207,6 +207,21 @@ class Handle:
         self._check(rc)
         return int(kb.value)
 
+    def get_tuning(self) -> dict:
+        """The handle's launch-shape knobs (mspai_get_tuning)."""
+        t = _lib.mspai_tuning()
+        self._check(self._lib.mspai_get_tuning(self._h, ctypes.byref(t)))
+        return {f: int(getattr(t, f)) for f, _ in _lib.mspai_tuning._fields_}
+
+    def set_tuning(self, **knobs) -> None:
+        """Sets some of the knobs (mspai_set_tuning checks the ranges)."""
+        t = _lib.mspai_tuning(**self.get_tuning())
+        for k, v in knobs.items():
+            if not hasattr(t, k):
+                raise ValueError(f"unknown tuning knob {k}")
+            setattr(t, k, int(v))
+        self._check(self._lib.mspai_set_tuning(self._h, ctypes.byref(t)))
+
     def nnz(self) -> int:
         v = ctypes.c_int64()
         self._check(self._lib.mspai_result_nnz(self._h, ctypes.byref(v)))

@@ -117,6 +117,9 @@ struct mspai_handle {
     size_t smem_budget = 48 * 1024;  // shared-memory area of each CTA solver (4 per SM)
     int fixed_arena = 107 * 1024;    // arena of the fixed-pattern solver's first launch (2 CTAs per SM)
     int fixed_arena_large = kFixedArenaLarge;  // ... and of its second launch
+    int warp_emax = 64;              // tiny bucket: entries of C(:, J_k) ...
+    int warp_nmax = 16;              // ... and |J_k|
+    int64_t w_smem_bytes = 96 * 1024;  // general solver: folded matrices up to this in smem
     bool used_fixed = false;         // the last setup ran the fixed-pattern solver
     int64_t list_len[kLists] = {};   // columns listed per work list in the last setup
 };
@@ -644,12 +647,12 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     rule.hi = col_hi;
     rule.single_bucket = prm->batched ? -1 : 2;
     rule.allow_warp = (adaptive || bs > 1) ? 0 : 1;
-    rule.warp_emax = 64;
-    rule.warp_nmax = 16;
+    rule.warp_emax = h->warp_emax;
+    rule.warp_nmax = h->warp_nmax;
     // fixed scalar patterns: every column beyond the warp bucket goes to the
     // fixed-pattern solver (bucket 1), which sizes its arrays per column
     const bool use_fixed = !adaptive && bs == 1 && prm->batched && !pb.qru;
-    rule.smem_w_bytes = use_fixed ? (int64_t(1) << 62) : 96 * 1024;
+    rule.smem_w_bytes = use_fixed ? (int64_t(1) << 62) : h->w_smem_bytes;
     rule.elem_bytes = elem;
     rule.grow_n = grow_n * bs;
     rule.grow_e = adaptive ? grow_n * bs * max_col_nnz : 0;
@@ -916,6 +919,40 @@ int mspai_tune(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, con
     h->r_valid = false;
     if (smem_kb_out)
         *smem_kb_out = best;
+    return MSPAI_OK;
+}
+
+int mspai_get_tuning(mspai_handle* h, mspai_tuning* t)
+{
+    if (!h || !t)
+        return h ? set_err(h, MSPAI_ERR_PARAM, "tuning is required") : MSPAI_ERR_STATE;
+    t->smem_kb = static_cast<int32_t>(h->smem_budget / 1024);
+    t->fixed_arena_kb = h->fixed_arena / 1024;
+    t->fixed_arena_large_kb = h->fixed_arena_large / 1024;
+    t->warp_emax = h->warp_emax;
+    t->warp_nmax = h->warp_nmax;
+    t->w_smem_kb = static_cast<int32_t>(h->w_smem_bytes / 1024);
+    return MSPAI_OK;
+}
+
+int mspai_set_tuning(mspai_handle* h, const mspai_tuning* t)
+{
+    if (!h || !t)
+        return h ? set_err(h, MSPAI_ERR_PARAM, "tuning is required") : MSPAI_ERR_STATE;
+    auto in = [](int v, int lo, int hi) { return v >= lo && v <= hi; };
+    if (!in(t->smem_kb, 16, 220) || !in(t->fixed_arena_kb, 8, 107) ||
+        !in(t->fixed_arena_large_kb, 8, 212) || !in(t->warp_emax, 16, 256) ||
+        !in(t->warp_nmax, 4, 32) || !in(t->w_smem_kb, 16, 220))
+        return set_err(h, MSPAI_ERR_PARAM,
+                       "tuning out of range: smem_kb 16..220, fixed_arena_kb 8..107, "
+                       "fixed_arena_large_kb 8..212, warp_emax 16..256, warp_nmax 4..32, "
+                       "w_smem_kb 16..220");
+    h->smem_budget = static_cast<size_t>(t->smem_kb) * 1024;
+    h->fixed_arena = t->fixed_arena_kb * 1024;
+    h->fixed_arena_large = t->fixed_arena_large_kb * 1024;
+    h->warp_emax = t->warp_emax;
+    h->warp_nmax = t->warp_nmax;
+    h->w_smem_bytes = static_cast<int64_t>(t->w_smem_kb) * 1024;
     return MSPAI_OK;
 }
 
