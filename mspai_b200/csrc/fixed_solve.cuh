@@ -82,6 +82,7 @@ struct FixShared {
     double tg_val[kFixMaxSpecial];
     int nspec;
     int mcount;                     // distinct rows of C(:, J)
+    int chol_fail;                  // a pivot of the Cholesky factorization was not positive
     int spec_e[kFixMaxSpecial];
     int spec_jj[kFixMaxSpecial];
     double spec_v[kFixMaxSpecial];
@@ -725,6 +726,119 @@ __device__ void fix_forward_substitute(const CtaGroup<NT>& g, const T* R, int n,
     }
 }
 
+// Cholesky factorization G = R^T R in place, R upper triangular in the packed
+// rows of fix_rs (row i holds columns i .. n - 1 of G's upper triangle on
+// entry, of R on return).  Right-looking by 16 columns: warp 0 factors the
+// diagonal block in registers (no CTA barrier inside); a thread per later
+// column solves R11^T X = G12 for its 16 entries; the trailing upper
+// triangle is updated by a thread per column.  Three barriers per block.
+// Returns false (uniformly) when a pivot is not positive (G not numerically
+// positive definite in T).  tile: 16 n elements, 16-byte aligned (the block
+// row of R right of the diagonal block, 16 consecutive values per column).
+template <class T, int NT>
+__device__ bool fix_cholesky(const CtaGroup<NT>& g, FixShared<T>& fs, T* R, int n, T* tile)
+{
+    const int tid = threadIdx.x, lane = tid & 31;
+    if (tid == 0)
+        fs.chol_fail = 0;
+    g.sync();
+    for (int c0 = 0; c0 < n; c0 += kFixPanel) {
+        const int nb = min(kFixPanel, n - c0);
+        if (tid < 32) {
+            // lane i < nb holds row c0 + i of the diagonal block (columns >= i)
+            T a[kFixPanel];
+#pragma unroll
+            for (int j = 0; j < kFixPanel; j++)
+                a[j] = (lane < nb && j >= lane && j < nb) ? R[fix_rs(c0 + lane, n) + (j - lane)]
+                                                          : T(0);
+            bool bad = false;
+#pragma unroll
+            for (int k = 0; k < kFixPanel; k++) {
+                if (k < nb) {
+                    const T piv = __shfl_sync(0xffffffffu, a[k], k);
+                    bad = bad || !(piv > T(0));
+                    const T rkk = bad ? T(1) : sqrt(piv);
+                    const T inv = T(1) / rkk;
+                    if (lane == k) {
+#pragma unroll
+                        for (int j = 0; j < kFixPanel; j++)
+                            a[j] = (j == k) ? rkk : (j > k ? a[j] * inv : a[j]);
+                    }
+                    // row k of R, broadcast; rows below subtract its outer product
+                    T rk[kFixPanel];
+#pragma unroll
+                    for (int j = 0; j < kFixPanel; j++)
+                        rk[j] = __shfl_sync(0xffffffffu, a[j], k);
+                    if (lane > k && lane < nb) {
+#pragma unroll
+                        for (int j = 0; j < kFixPanel; j++)
+                            if (j >= lane)
+                                a[j] -= rk[lane] * rk[j];
+                    }
+                }
+            }
+            if (lane < nb) {
+#pragma unroll
+                for (int j = 0; j < kFixPanel; j++)
+                    if (j >= lane && j < nb)
+                        R[fix_rs(c0 + lane, n) + (j - lane)] = a[j];
+            }
+            if (lane == 0 && bad)
+                fs.chol_fail = 1;
+        }
+        g.sync();
+        if (fs.chol_fail)
+            return false;  // uniform: read after the barrier
+        const int c1 = c0 + nb;
+        // R(c0:c1, j) for j >= c1: forward substitution with R11^T, one column per thread
+        for (int j = c1 + tid; j < n; j += NT) {
+            T x[kFixPanel];
+#pragma unroll
+            for (int i = 0; i < kFixPanel; i++) {
+                if (i < nb) {
+                    const T* ri = R + fix_rs(c0 + i, n) - (c0 + i);  // ri[c] = R(c0 + i, c)
+                    T v = ri[j];
+#pragma unroll
+                    for (int l = 0; l < kFixPanel; l++)
+                        if (l < i)
+                            v -= R[fix_rs(c0 + l, n) + (c0 + i - c0 - l)] * x[l];
+                    x[i] = v / ri[c0 + i];
+                }
+            }
+            T* tj = tile + static_cast<size_t>(j - c1) * kFixPanel;
+#pragma unroll
+            for (int i = 0; i < kFixPanel; i++) {
+                if (i < nb)
+                    R[fix_rs(c0 + i, n) + (j - c0 - i)] = x[i];
+                tj[i] = (i < nb) ? x[i] : T(0);
+            }
+        }
+        g.sync();
+        // trailing update G(i, j) -= sum_l R(c0 + l, i) R(c0 + l, j), c1 <= i <= j < n;
+        // a thread per column j keeps R(c0 + l, j) in registers, column i's 16
+        // values come from the tile (broadcast: the threads of a warp are at
+        // the same i)
+        for (int j = c1 + tid; j < n; j += NT) {
+            T rj[kFixPanel];
+            fix_load16(tile + static_cast<size_t>(j - c1) * kFixPanel, rj);
+            T* gj = R + j;  // gj[fix_rs(i, n) - i] = G(i, j)
+            for (int i = c1; i <= j; i++) {
+                T v[kFixPanel];
+                fix_load16(tile + static_cast<size_t>(i - c1) * kFixPanel, v);
+                T s0 = T(0), s1 = T(0);
+#pragma unroll
+                for (int l = 0; l < kFixPanel; l += 2) {
+                    s0 += v[l] * rj[l];
+                    s1 += v[l + 1] * rj[l + 1];
+                }
+                gj[fix_rs(i, n) - i] -= s0 + s1;
+            }
+        }
+        g.sync();
+    }
+    return true;
+}
+
 // Inverses of the 16 x 16 diagonal blocks of R (packed rows, fix_rs), block b
 // at Dinv + 256 b, column-major (D(r, c) at r + 16 c, zero below the
 // diagonal).  Thread (b, i) solves U x = e_i for column i of block b.  R must
@@ -1260,6 +1374,80 @@ __device__ bool fixed_solve_column(const CtaGroup<NT>& g, FixShared<T>& fs, cons
                 }
             }
             g.sync();  // every thread is done with the kept factor's arrays
+        }
+    }
+
+    // ---- mixed mode: R from the Cholesky factorization of C^T C, formed in
+    // T from the sparse entries (the folded diagonal in FP64), then the FP64
+    // refinement from x = 0 (its first step is the normal-equations solve).
+    // The factor only preconditions the refinement: R^T R equals C^T C to
+    // O(u_T ||C||^2), as the R of the Householder QR in T does, so the
+    // corrections contract alike; the refinement ends at the least-squares
+    // solution in FP64.  A column whose Cholesky meets a pivot <= 0 or whose
+    // refinement does not converge takes the Householder path below.  (FP64
+    // mode has no refinement and keeps the Householder QR.)
+    if constexpr (sizeof(T) == 4) if (pb.refine > 0) {
+        FixArena b2 = a;
+        b2.hi = arena_cap;  // the transient arrays are dead
+        const int r_el = fix_rs(n, n);
+        const int nblk = (n + kFixPanel - 1) / kFixPanel;
+        T* gv = b2.low<T>(n);
+        T* Gs = b2.low<T>(r_el);
+        T* tile = b2.low<T>(kFixPanel * n);
+        T* Dr = b2.low<T>(kFixPanel * kFixPanel * nblk);
+        if (b2.ok()) {
+            // G = C^T C: column j of G's lower triangle (= row j of its upper
+            // triangle, packed as R) by one thread, in entry order
+            for (int j = tid; j < n; j += NT) {
+                T* row = Gs + fix_rs(j, n) - j;  // row[c] = G(j, c), c >= j
+                for (int c = j; c <= n; c++)
+                    row[c] = T(0);
+                double dd = d0sq[j];
+                for (int sp = 0; sp < nspec; sp++)
+                    if (fs.spec_jj[sp] == j)
+                        dd += fs.spec_v[sp] * fs.spec_v[sp];
+                for (int q = cstart[j]; q < cstart[j + 1]; q++) {
+                    const double vq = csh_v[q];
+                    const int grp_s = sof[csh_d[q]];
+                    for (int t = gstart[grp_s]; t < gstart[grp_s + 1]; t++) {
+                        const int q2 = rq[t];
+                        const int j2 = csh_jj[q2];
+                        if (j2 > j)
+                            row[j2] += static_cast<T>(vq * csh_v[q2]);
+                        else if (j2 == j)
+                            dd += vq * csh_v[q2];
+                    }
+                }
+                row[j] = static_cast<T>(dd);
+            }
+            g.sync();
+            if (fix_cholesky<T, NT>(g, fs, Gs, n, tile)) {
+                fix_invert_diag<T, NT>(Gs, n, Dr);
+                for (int t = tid; t < n; t += NT)
+                    x[t] = 0.0;
+                g.sync();
+                double r2 = residual(true, gv);  // gv = C^T b
+                ref_steps = 0;
+                if (refine(Gs, Dr, gv, pb.refine + 2, r2)) {
+                    if (out.rstore) {
+                        T* dst = static_cast<T*>(out.rstore) + out.roff[col];
+                        for (int t = tid; t < n * (n + 1) / 2; t += NT) {
+                            int j = static_cast<int>((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
+                            while (j * (j + 1) / 2 > t)
+                                j--;
+                            while ((j + 1) * (j + 2) / 2 <= t)
+                                j++;
+                            const int i = t - j * (j + 1) / 2;
+                            dst[t] = Gs[fix_rs(i, n) + (j - i)];
+                        }
+                    }
+                    const double dn = n;
+                    finish(r2, 0,
+                           dn * dn * dn / 3.0 + 2.0 * SEn + ref_steps * (2.0 * dn * dn + 4.0 * SEn));
+                    return true;
+                }
+            }
+            g.sync();  // every thread is done with the factor's arrays
         }
     }
 
