@@ -1421,14 +1421,20 @@ __device__ bool fixed_solve_column(const CtaGroup<NT>& g, FixShared<T>& fs, cons
                 row[j] = static_cast<T>(dd);
             }
             g.sync();
-            if (fix_cholesky<T, NT>(g, fs, Gs, n, tile)) {
+            PHASE_MARK(2);
+            const bool factored = fix_cholesky<T, NT>(g, fs, Gs, n, tile);
+            PHASE_MARK(3);
+            if (factored) {
                 fix_invert_diag<T, NT>(Gs, n, Dr);
                 for (int t = tid; t < n; t += NT)
                     x[t] = 0.0;
                 g.sync();
+                PHASE_MARK(6);
                 double r2 = residual(true, gv);  // gv = C^T b
                 ref_steps = 0;
-                if (refine(Gs, Dr, gv, pb.refine + 2, r2)) {
+                const bool conv = refine(Gs, Dr, gv, pb.refine + 2, r2);
+                PHASE_MARK(7);
+                if (conv) {
                     if (out.rstore) {
                         T* dst = static_cast<T*>(out.rstore) + out.roff[col];
                         for (int t = tid; t < n * (n + 1) / 2; t += NT) {
