@@ -74,6 +74,24 @@ int mspai_block_pattern_generate(const mspai_csc* C, int32_t bs, int32_t kind,
                                  mspai_matrix* P_out);
 
 /*
+ * The reference's power pattern with its count-based sparsification
+ * (To_Pattern_Powers, src/Matrix.imp:359-470, there through PETSc): with
+ * S = Sparsify(|A|), then nb_pw times { S = Sparsify(S) (from the second
+ * time on); S = S S }, then S = Sparsify(S), P = pattern(S).  Sparsify
+ * (src/Matrix.imp:471-620) keeps in column k the lfill_k = nnz(A(:, k))
+ * largest entries by magnitude, every entry equal in magnitude to the
+ * smallest kept one, and the diagonal (which takes the place of the smallest
+ * kept entry when it is not among them; value 0 when absent).  Equal
+ * magnitudes are ordered by row (a stable sort of the row-ordered column).
+ * A square on the host with values, 0 <= nb_pw <= 4; computed on GPU
+ * `device`; P_out owned (mspai_matrix_free), its values the magnitudes of S.
+ * A column may hold at most 8192 products or entries, else
+ * MSPAI_ERR_CAPACITY.
+ */
+int mspai_pattern_powers(const mspai_csc* A, int32_t nb_pw, int32_t device, mspai_matrix* P_out,
+                         char* msg, int32_t msg_len);
+
+/*
  * Start pattern from the square of A (the first n rows of C), computed on
  * GPU `device`: P(:, k) = { i : |(A^2)(i, k)| >= drop * max_i |(A^2)(i, k)| }
  * (drop = 0 keeps the whole pattern of A^2).  The family of the reference's

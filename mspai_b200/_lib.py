@@ -73,7 +73,7 @@ EXPORTED = [
     "mspai_matrix_view", "mspai_matrix_free", "mspai_mm_read", "mspai_mm_write",
     "mspai_probing_assemble", "mspai_pattern_generate", "mspai_row_structure",
     "mspai_measure_fma_peak", "mspai_setup_fixed_noalloc", "mspai_block_pattern_generate",
-    "mspai_pattern_power2", "mspai_get_tuning", "mspai_set_tuning",
+    "mspai_pattern_power2", "mspai_get_tuning", "mspai_set_tuning", "mspai_pattern_powers",
 ]
 
 _lib = None
@@ -155,6 +155,9 @@ def load() -> ctypes.CDLL:
     lib.mspai_pattern_power2.argtypes = [P(mspai_csc), ctypes.c_double, ctypes.c_int32,
                                          P(mspai_matrix), ctypes.c_char_p, ctypes.c_int32]
     lib.mspai_pattern_power2.restype = I
+    lib.mspai_pattern_powers.argtypes = [P(mspai_csc), ctypes.c_int32, ctypes.c_int32,
+                                         P(mspai_matrix), ctypes.c_char_p, ctypes.c_int32]
+    lib.mspai_pattern_powers.restype = I
     lib.mspai_row_structure.argtypes = [P(mspai_csc), ctypes.c_int32, P(mspai_matrix)]
     lib.mspai_row_structure.restype = I
     _lib = lib

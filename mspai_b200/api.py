@@ -424,6 +424,24 @@ def pattern_power2(C: sp.spmatrix, drop: float = 1e-3, device: int = 0) -> sp.cs
         lib.mspai_matrix_free(ctypes.byref(m))
 
 
+def pattern_powers(A: sp.spmatrix, nb_pw: int = 1, device: int = 0) -> sp.csc_matrix:
+    """The reference's power pattern with its count-based Sparsify
+    (mspai_pattern_powers, To_Pattern_Powers): a CSC matrix whose pattern is
+    P and whose values are the magnitudes of the sparsified powers."""
+    lib = _lib.load()
+    s = _Staged(A, False)
+    m = _lib.mspai_matrix()
+    buf = ctypes.create_string_buffer(512)
+    rc = lib.mspai_pattern_powers(ctypes.byref(s.c), int(nb_pw), int(device), ctypes.byref(m),
+                                  buf, len(buf))
+    if rc != _lib.MSPAI_OK:
+        raise MspaiError(rc, buf.value.decode(errors="replace"))
+    try:
+        return _owned_to_scipy(m)
+    finally:
+        lib.mspai_matrix_free(ctypes.byref(m))
+
+
 def block_pattern(C: sp.spmatrix, bs: int, kind: Union[int, str]) -> sp.csc_matrix:
     """Block start pattern (n/bs x n/bs): -1 / "diag" diagonal blocks, -2 / "A"
     the block pattern of C's first n rows (mspai_block_pattern_generate)."""
