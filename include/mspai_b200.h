@@ -201,6 +201,10 @@ typedef struct {
     int32_t warp_nmax;            /* ... and |J_k| at most this, 4..32 (16)             */
     int32_t w_smem_kb;            /* general solver: a column whose folded matrix fits
                                      this goes to the shared-memory bucket, 16..220 (96) */
+    int32_t warp_emax_adaptive;   /* adaptive scalar setups: a warp per column (slots in
+                                     global memory) when the entries after the pattern
+                                     updates are at most this, 16..4096 (256) ...       */
+    int32_t warp_nmax_adaptive;   /* ... and |J_k| after the updates at most this, 4..64 (32) */
 } mspai_tuning;
 
 int mspai_get_tuning(mspai_handle* h, mspai_tuning* t);

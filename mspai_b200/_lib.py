@@ -54,7 +54,8 @@ class mspai_stats(ctypes.Structure):
 class mspai_tuning(ctypes.Structure):
     _fields_ = [("smem_kb", ctypes.c_int32), ("fixed_arena_kb", ctypes.c_int32),
                 ("fixed_arena_large_kb", ctypes.c_int32), ("warp_emax", ctypes.c_int32),
-                ("warp_nmax", ctypes.c_int32), ("w_smem_kb", ctypes.c_int32)]
+                ("warp_nmax", ctypes.c_int32), ("w_smem_kb", ctypes.c_int32),
+                ("warp_emax_adaptive", ctypes.c_int32), ("warp_nmax_adaptive", ctypes.c_int32)]
 
 
 class mspai_matrix(ctypes.Structure):

@@ -120,6 +120,8 @@ struct mspai_handle {
     int warp_emax = 64;              // tiny bucket: entries of C(:, J_k) ...
     int warp_nmax = 16;              // ... and |J_k|
     int64_t w_smem_bytes = 96 * 1024;  // general solver: folded matrices up to this in smem
+    int warp_emax_adaptive = 256;    // adaptive tiny bucket (warp per column, global slots)
+    int warp_nmax_adaptive = 32;
     bool used_fixed = false;         // the last setup ran the fixed-pattern solver
     int64_t list_len[kLists] = {};   // columns listed per work list in the last setup
 };
@@ -646,9 +648,11 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     rule.lo = col_lo;
     rule.hi = col_hi;
     rule.single_bucket = prm->batched ? -1 : 2;
-    rule.allow_warp = (adaptive || bs > 1) ? 0 : 1;
-    rule.warp_emax = h->warp_emax;
-    rule.warp_nmax = h->warp_nmax;
+    // tiny bucket: a warp per column (adaptive scalar setups too, with the
+    // slots in global memory; not with the QR-update state)
+    rule.allow_warp = (bs > 1 || pb.qru) ? 0 : 1;
+    rule.warp_emax = adaptive ? h->warp_emax_adaptive : h->warp_emax;
+    rule.warp_nmax = adaptive ? h->warp_nmax_adaptive : h->warp_nmax;
     // fixed scalar patterns: every column beyond the warp bucket goes to the
     // fixed-pattern solver (bucket 1), which sizes its arrays per column
     const bool use_fixed = !adaptive && bs == 1 && prm->batched && !pb.qru;
@@ -728,10 +732,24 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
         if (fp64_bucket)
             pbb.refine = 0;
         bool use_warp = (b == 0);
-        if (use_warp &&
-            mspai::warp_slot_bytes(cap, elem_b) * (mspai::kWarpKernelThreads / 32) > 200 * 1024)
-            use_warp = false;
-        if (use_warp) {
+        const bool warp_global =
+            use_warp && (adaptive || mspai::warp_slot_bytes(cap, elem_b) *
+                                             (mspai::kWarpKernelThreads / 32) > 200 * 1024);
+        if (warp_global) {
+            const size_t need = mspai::warp_global_scratch_bytes(cap, elem_b, count);
+            CUDA_TRY(h, h->scratch.ensure(need));
+            if (adaptive)  // the candidate bit vectors of the slots start cleared
+                CUDA_TRY(h, cudaMemsetAsync(h->scratch.p, 0, need, st));
+            CUDA_TRY(h, cudaEventRecord(h->evb[0], st));
+            h->launches++;
+            CUDA_TRY(h, mspai::launch_warp_solve_global(elem_b, pbb, cap, out, list, count,
+                                                        counter, h->scratch.as<char>(),
+                                                        h->scratch.bytes, st, &grid));
+            CUDA_TRY(h, cudaEventRecord(h->evb[1], st));
+            timed[0] = true;
+            h->stats.bucket_columns[0] = count;
+        }
+        else if (use_warp) {
             CUDA_TRY(h, cudaEventRecord(h->evb[0], st));
             h->launches++;
             CUDA_TRY(h, mspai::launch_warp_solve(elem_b, pbb, cap, out, list, count, counter, st,
@@ -932,6 +950,8 @@ int mspai_get_tuning(mspai_handle* h, mspai_tuning* t)
     t->warp_emax = h->warp_emax;
     t->warp_nmax = h->warp_nmax;
     t->w_smem_kb = static_cast<int32_t>(h->w_smem_bytes / 1024);
+    t->warp_emax_adaptive = h->warp_emax_adaptive;
+    t->warp_nmax_adaptive = h->warp_nmax_adaptive;
     return MSPAI_OK;
 }
 
@@ -942,17 +962,21 @@ int mspai_set_tuning(mspai_handle* h, const mspai_tuning* t)
     auto in = [](int v, int lo, int hi) { return v >= lo && v <= hi; };
     if (!in(t->smem_kb, 16, 220) || !in(t->fixed_arena_kb, 8, 107) ||
         !in(t->fixed_arena_large_kb, 8, 212) || !in(t->warp_emax, 16, 256) ||
-        !in(t->warp_nmax, 4, 32) || !in(t->w_smem_kb, 16, 220))
+        !in(t->warp_nmax, 4, 32) || !in(t->w_smem_kb, 16, 220) ||
+        !in(t->warp_emax_adaptive, 16, 4096) || !in(t->warp_nmax_adaptive, 4, 64))
         return set_err(h, MSPAI_ERR_PARAM,
                        "tuning out of range: smem_kb 16..220, fixed_arena_kb 8..107, "
                        "fixed_arena_large_kb 8..212, warp_emax 16..256, warp_nmax 4..32, "
-                       "w_smem_kb 16..220");
+                       "w_smem_kb 16..220, warp_emax_adaptive 16..4096, "
+                       "warp_nmax_adaptive 4..64");
     h->smem_budget = static_cast<size_t>(t->smem_kb) * 1024;
     h->fixed_arena = t->fixed_arena_kb * 1024;
     h->fixed_arena_large = t->fixed_arena_large_kb * 1024;
     h->warp_emax = t->warp_emax;
     h->warp_nmax = t->warp_nmax;
     h->w_smem_bytes = static_cast<int64_t>(t->w_smem_kb) * 1024;
+    h->warp_emax_adaptive = t->warp_emax_adaptive;
+    h->warp_nmax_adaptive = t->warp_nmax_adaptive;
     return MSPAI_OK;
 }
 

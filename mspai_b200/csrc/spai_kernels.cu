@@ -115,6 +115,33 @@ __global__ void __launch_bounds__(kWarpKernelThreads)
     }
 }
 
+// A warp per column with the slot in global memory (scratch + slot_bytes per
+// warp): the tiny bucket of adaptive setups, whose candidate bit vector over
+// all problem columns does not fit a shared-memory slot.
+template <class T>
+__global__ void __launch_bounds__(kWarpKernelThreads)
+    warp_solve_global_kernel(Problem pb, Caps cap, Output out, const int32_t* __restrict__ list,
+                             int count, int32_t* __restrict__ counter, char* __restrict__ scratch,
+                             size_t slot_bytes)
+{
+    __shared__ GroupScratch sc[kWarpKernelThreads / 32];
+    const int w = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    WarpGroup g{&sc[w]};
+    SlotLayout<T> lay(cap, false);
+    const size_t slot_id = static_cast<size_t>(blockIdx.x) * (kWarpKernelThreads / 32) + w;
+    Slot<T> s = lay.at(scratch + slot_id * slot_bytes, nullptr);
+    while (true) {
+        int t = 0;
+        if (lane == 0)
+            t = atomicAdd(counter, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= count)
+            break;
+        solve_column<T>(g, pb, cap, s, out, list[t]);
+    }
+}
+
 // The solver is latency bound: throughput grows with the columns in flight
 // per SM.  MINB CTAs of 128 threads per SM bound the registers per thread
 // (128 for 4, 64 for 8); the shared-memory area per CTA is chosen with it.
@@ -431,6 +458,50 @@ static cudaError_t launch_warp_t(const Problem& pb, const Caps& cap, const Outpu
     warp_solve_kernel<T><<<grid, kWarpKernelThreads, smem, st>>>(pb, cap, out, list, count,
                                                                    counter, slot);
     return cudaGetLastError();
+}
+
+template <class T>
+static int warp_global_grid(int count)
+{
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, warp_solve_global_kernel<T>,
+                                                  kWarpKernelThreads, 0);
+    const int need = (count + kWarpKernelThreads / 32 - 1) / (kWarpKernelThreads / 32);
+    return std::max(1, std::min(std::max(per_sm, 1) * num_sms(), need));
+}
+
+size_t warp_global_scratch_bytes(const Caps& cap, int elem_bytes, int count)
+{
+    const int grid = elem_bytes == 4 ? warp_global_grid<float>(count) : warp_global_grid<double>(count);
+    return warp_slot_bytes(cap, elem_bytes) * static_cast<size_t>(grid) * (kWarpKernelThreads / 32);
+}
+
+template <class T>
+static cudaError_t launch_warp_global_t(const Problem& pb, const Caps& cap, const Output& out,
+                                        const int32_t* list, int count, int32_t* counter,
+                                        char* scratch, size_t scratch_bytes, cudaStream_t st,
+                                        int* grid_out)
+{
+    const size_t slot = SlotLayout<T>(cap, false).bytes;
+    int grid = warp_global_grid<T>(count);
+    grid = std::max(1, std::min<int>(grid, static_cast<int>(
+                                               scratch_bytes / (slot * (kWarpKernelThreads / 32)))));
+    *grid_out = grid;
+    warp_solve_global_kernel<T><<<grid, kWarpKernelThreads, 0, st>>>(pb, cap, out, list, count,
+                                                                     counter, scratch, slot);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_warp_solve_global(int elem_bytes, const Problem& pb, const Caps& cap,
+                                     const Output& out, const int32_t* list, int count,
+                                     int32_t* counter, char* scratch, size_t scratch_bytes,
+                                     cudaStream_t st, int* grid_out)
+{
+    if (elem_bytes == 4)
+        return launch_warp_global_t<float>(pb, cap, out, list, count, counter, scratch,
+                                           scratch_bytes, st, grid_out);
+    return launch_warp_global_t<double>(pb, cap, out, list, count, counter, scratch,
+                                        scratch_bytes, st, grid_out);
 }
 
 cudaError_t launch_warp_solve(int elem_bytes, const Problem& pb, const Caps& cap,

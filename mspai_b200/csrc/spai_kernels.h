@@ -55,6 +55,13 @@ cudaError_t launch_bucket(const int32_t* E, const int32_t* nk, int n, const Buck
                           int32_t* counts, int32_t* maxE, int32_t* maxN, int32_t* lists,
                           cudaStream_t st);
 size_t warp_slot_bytes(const Caps& cap, int elem_bytes);
+// warp per column with the slots in global memory (scratch of
+// warp_global_scratch_bytes; adaptive setups: cleared before the launch)
+size_t warp_global_scratch_bytes(const Caps& cap, int elem_bytes, int count);
+cudaError_t launch_warp_solve_global(int elem_bytes, const Problem& pb, const Caps& cap,
+                                     const Output& out, const int32_t* list, int count,
+                                     int32_t* counter, char* scratch, size_t scratch_bytes,
+                                     cudaStream_t st, int* grid_out);
 size_t cta_slot_bytes(const Caps& cap, int elem_bytes, bool w_smem);
 size_t w_bytes(const Caps& cap, int elem_bytes);
 // CTAs per SM of the solver for this element size and shared-memory area
