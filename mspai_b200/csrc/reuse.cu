@@ -9,7 +9,9 @@
 //   |J_k|; for every j in J_k (sorted): j - k, nnz(C(:,j)), and every entry
 //   (row, value) of C(:,j); then every entry of B(:,k) when B is given.
 // Rows below n are written relative to k (r - k); probing rows (r >= n) are
-// written absolute, since they do not move with k.  Two columns with equal
+// written absolute, since they do not move with k.  A block problem column k
+// (fixed block patterns, bs > 1) streams its bs scalar columns per block of
+// J_k, relative to its first scalar column bs k, and B's bs columns.  Two columns with equal
 // streams have the same I_k - k, J_k - k, the same Â (same row and column
 // order) and the same right-hand side, so the same solution, bit for bit.
 // Equal streams are a sufficient condition for equal Â: columns whose Â agree
@@ -60,37 +62,45 @@ __device__ __forceinline__ uint64_t dbits(double v)
     return static_cast<uint64_t>(__double_as_longlong(v));
 }
 
-// tags: (jj + 1) << 32 | 2 * t (+1 for the value) for entry t of the jj-th
-// column of J; jj = n_k for the entries of B(:,k); (jj + 1) << 32 | 0xffffffff
-// for the column header (j - k, nnz); 0 for |J_k|
+// tags: (q + 1) << 32 | 2 * t (+1 for the value) for entry t of the q-th
+// scalar column of J (q = bs jj + c for the c-th scalar column of the jj-th
+// block of J); q = bs n_k + c for the entries of B(:, bs k + c);
+// (q + 1) << 32 | 0xffffffff for a column's header (j - bs k, nnz); 0 for |J_k|.
+// Rows below n are relative to bs k, the first scalar column of problem k.
 __device__ uint64_t column_hash(const Problem& pb, int k, int lane)
 {
+    const int bs = pb.bs;
     const int64_t p0 = pb.pptr[k], p1 = pb.pptr[k + 1];
     const int nk = static_cast<int>(p1 - p0);
+    const int k0 = bs * k;
     uint64_t h = (lane == 0) ? tagged(static_cast<uint64_t>(nk), 0) : 0;
     for (int jj = 0; jj < nk; jj++) {
-        const int j = pb.pidx[p0 + jj];
-        const int64_t c0 = pb.cptr[j], c1 = pb.cptr[j + 1];
-        const uint64_t base = static_cast<uint64_t>(jj + 1) << 32;
-        if (lane == 0)
-            h += tagged((static_cast<uint64_t>(static_cast<int64_t>(j) - k) << 32) ^
-                            static_cast<uint64_t>(c1 - c0),
-                        base | 0xffffffffull);
-        for (int64_t e = c0 + lane; e < c1; e += 32) {
-            const uint64_t t = static_cast<uint64_t>(e - c0);
-            h += tagged(enc_row(pb.cidx[e], k, pb.n), base | (2 * t));
-            h += tagged(dbits(pb.cval[e]), base | (2 * t + 1));
+        for (int c = 0; c < bs; c++) {
+            const int j = bs * pb.pidx[p0 + jj] + c;
+            const int64_t c0 = pb.cptr[j], c1 = pb.cptr[j + 1];
+            const uint64_t base = static_cast<uint64_t>(bs * jj + c + 1) << 32;
+            if (lane == 0)
+                h += tagged((static_cast<uint64_t>(static_cast<int64_t>(j) - k0) << 32) ^
+                                static_cast<uint64_t>(c1 - c0),
+                            base | 0xffffffffull);
+            for (int64_t e = c0 + lane; e < c1; e += 32) {
+                const uint64_t t = static_cast<uint64_t>(e - c0);
+                h += tagged(enc_row(pb.cidx[e], k0, pb.n), base | (2 * t));
+                h += tagged(dbits(pb.cval[e]), base | (2 * t + 1));
+            }
         }
     }
     if (pb.bptr) {
-        const int64_t b0 = pb.bptr[k], b1 = pb.bptr[k + 1];
-        const uint64_t base = static_cast<uint64_t>(nk + 1) << 32;
-        if (lane == 0)
-            h += tagged(static_cast<uint64_t>(b1 - b0), base | 0xffffffffull);
-        for (int64_t e = b0 + lane; e < b1; e += 32) {
-            const uint64_t t = static_cast<uint64_t>(e - b0);
-            h += tagged(enc_row(pb.bidx[e], k, pb.n), base | (2 * t));
-            h += tagged(dbits(pb.bval[e]), base | (2 * t + 1));
+        for (int c = 0; c < bs; c++) {
+            const int64_t b0 = pb.bptr[k0 + c], b1 = pb.bptr[k0 + c + 1];
+            const uint64_t base = static_cast<uint64_t>(bs * nk + c + 1) << 32;
+            if (lane == 0)
+                h += tagged(static_cast<uint64_t>(b1 - b0), base | 0xffffffffull);
+            for (int64_t e = b0 + lane; e < b1; e += 32) {
+                const uint64_t t = static_cast<uint64_t>(e - b0);
+                h += tagged(enc_row(pb.bidx[e], k0, pb.n), base | (2 * t));
+                h += tagged(dbits(pb.bval[e]), base | (2 * t + 1));
+            }
         }
     }
 #pragma unroll
@@ -99,40 +109,44 @@ __device__ uint64_t column_hash(const Problem& pb, int k, int lane)
     return h | 1ull;  // 0 marks an empty slot
 }
 
-// 1 if the streams of columns a and b are equal (warp-uniform result)
+// 1 if the entries of scalar columns ja (problem a) and jb (problem b) are
+// equal relative to their problems' first scalar columns a0, b0 (warp-uniform)
+__device__ int same_entries(const int64_t* ptr, const int32_t* idx, const double* val, int ja,
+                            int jb, int a0, int b0, int n, int lane)
+{
+    const int64_t s0 = ptr[ja], t0 = ptr[jb];
+    const int64_t len = ptr[ja + 1] - s0;
+    if (len != ptr[jb + 1] - t0)
+        return 0;
+    int diff = 0;
+    for (int64_t t = lane; t < len; t += 32)
+        diff |= (enc_row(idx[s0 + t], a0, n) != enc_row(idx[t0 + t], b0, n)) ||
+                (dbits(val[s0 + t]) != dbits(val[t0 + t]));
+    return __any_sync(0xffffffffu, diff) ? 0 : 1;
+}
+
+// 1 if the streams of problem columns a and b are equal (warp-uniform result)
 __device__ int same_stream(const Problem& pb, int a, int b, int lane)
 {
+    const int bs = pb.bs;
     const int64_t pa = pb.pptr[a], pbb = pb.pptr[b];
     const int na = static_cast<int>(pb.pptr[a + 1] - pa);
     if (na != static_cast<int>(pb.pptr[b + 1] - pbb))
         return 0;
+    const int a0 = bs * a, b0 = bs * b;
     for (int jj = 0; jj < na; jj++) {
         const int ja = pb.pidx[pa + jj], jb = pb.pidx[pbb + jj];
         if (static_cast<int64_t>(ja) - a != static_cast<int64_t>(jb) - b)
             return 0;
-        const int64_t a0 = pb.cptr[ja], b0 = pb.cptr[jb];
-        const int64_t len = pb.cptr[ja + 1] - a0;
-        if (len != pb.cptr[jb + 1] - b0)
-            return 0;
-        int diff = 0;
-        for (int64_t t = lane; t < len; t += 32)
-            diff |= (enc_row(pb.cidx[a0 + t], a, pb.n) != enc_row(pb.cidx[b0 + t], b, pb.n)) ||
-                    (dbits(pb.cval[a0 + t]) != dbits(pb.cval[b0 + t]));
-        if (__any_sync(0xffffffffu, diff))
-            return 0;
+        for (int c = 0; c < bs; c++)
+            if (!same_entries(pb.cptr, pb.cidx, pb.cval, bs * ja + c, bs * jb + c, a0, b0, pb.n,
+                              lane))
+                return 0;
     }
-    if (pb.bptr) {
-        const int64_t a0 = pb.bptr[a], b0 = pb.bptr[b];
-        const int64_t len = pb.bptr[a + 1] - a0;
-        if (len != pb.bptr[b + 1] - b0)
-            return 0;
-        int diff = 0;
-        for (int64_t t = lane; t < len; t += 32)
-            diff |= (enc_row(pb.bidx[a0 + t], a, pb.n) != enc_row(pb.bidx[b0 + t], b, pb.n)) ||
-                    (dbits(pb.bval[a0 + t]) != dbits(pb.bval[b0 + t]));
-        if (__any_sync(0xffffffffu, diff))
-            return 0;
-    }
+    if (pb.bptr)
+        for (int c = 0; c < bs; c++)
+            if (!same_entries(pb.bptr, pb.bidx, pb.bval, a0 + c, b0 + c, a0, b0, pb.n, lane))
+                return 0;
     return 1;
 }
 
@@ -206,7 +220,8 @@ __global__ void reuse_verify_kernel(Problem pb, int nprob, ReuseTable t, int32_t
         atomicAdd(nreused, mine);
 }
 
-__global__ void reuse_copy_kernel(const int32_t* __restrict__ rep, int nprob, Output out)
+__global__ void reuse_copy_kernel(const int32_t* __restrict__ rep, int nprob, int bs,
+                                  Output out)
 {
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
@@ -214,19 +229,27 @@ __global__ void reuse_copy_kernel(const int32_t* __restrict__ rep, int nprob, Ou
         const int r = rep[k];
         if (r == k)
             continue;
-        const int64_t dst = out.optr[k], src = out.optr[r];
-        const int len = out.olen[r];
-        for (int t = lane; t < len; t += 32)
-            out.oval[dst + t] = out.oval[src + t];
-        if (lane == 0) {
-            out.olen[k] = len;
-            out.res[k] = out.res[r];
-            out.steps[k] = out.steps[r];
-            out.status[k] = out.status[r];
-            // the work was done once, for the representative
-            out.work[3 * static_cast<size_t>(k)] = 0.0;
-            out.work[3 * static_cast<size_t>(k) + 1] = 0.0;
-            out.work[3 * static_cast<size_t>(k) + 2] = 0.0;
+        // the bs scalar columns of the problem; a block problem's rows move
+        // with it (J_k = J_r + (k - r) blocks)
+        for (int c = 0; c < bs; c++) {
+            const int sk = bs * k + c, sr = bs * r + c;
+            const int64_t dst = out.optr[sk], src = out.optr[sr];
+            const int len = out.olen[sr];
+            for (int t = lane; t < len; t += 32) {
+                out.oval[dst + t] = out.oval[src + t];
+                if (out.write_idx)
+                    out.oidx[dst + t] = out.oidx[src + t] + bs * (k - r);
+            }
+            if (lane == 0) {
+                out.olen[sk] = len;
+                out.res[sk] = out.res[sr];
+                out.steps[sk] = out.steps[sr];
+                out.status[sk] = out.status[sr];
+                // the work was done once, for the representative
+                out.work[3 * static_cast<size_t>(sk)] = 0.0;
+                out.work[3 * static_cast<size_t>(sk) + 1] = 0.0;
+                out.work[3 * static_cast<size_t>(sk) + 2] = 0.0;
+            }
         }
     }
 }
@@ -270,11 +293,12 @@ cudaError_t launch_reuse_keys(const Problem& pb, int nprob, const ReuseTable& t,
     return cudaGetLastError();
 }
 
-cudaError_t launch_reuse_copy(const int32_t* rep, int nprob, const Output& out, cudaStream_t st)
+cudaError_t launch_reuse_copy(const int32_t* rep, int nprob, int bs, const Output& out,
+                              cudaStream_t st)
 {
     if (nprob <= 0)
         return cudaSuccess;
-    reuse_copy_kernel<<<grid_for(nprob), 256, 0, st>>>(rep, nprob, out);
+    reuse_copy_kernel<<<grid_for(nprob), 256, 0, st>>>(rep, nprob, bs, out);
     return cudaGetLastError();
 }
 

@@ -619,9 +619,9 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
     h->launches++;
     CUDA_TRY(h, mspai::launch_plan(pb.cptr, pb.pptr, pb.pidx, nprob, bs, h->E.as<int32_t>(),
                                    h->nk.as<int32_t>(), st));
-    // ---- reuse of identical problems (-cs / -ch): fixed scalar patterns
-    // (not with keep_factors: a reused column has no factor of its own)
-    const bool reuse = (prm->cs > 0 || prm->ch > 0) && !adaptive && bs == 1 && prm->batched &&
+    // ---- reuse of identical problems (-cs / -ch): fixed scalar and block
+    // patterns (not with keep_factors: a reused column has no factor of its own)
+    const bool reuse = (prm->cs > 0 || prm->ch > 0) && !adaptive && prm->batched &&
                        !partial && !prm->keep_factors;
     int32_t* drep = nullptr;
     if (reuse) {
@@ -813,7 +813,7 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
 
     if (reuse) {
         h->launches++;
-        CUDA_TRY(h, mspai::launch_reuse_copy(drep, nprob, out, st));
+        CUDA_TRY(h, mspai::launch_reuse_copy(drep, nprob, bs, out, st));
     }
 
     // ---- assemble M

@@ -122,7 +122,8 @@ size_t reuse_table_slots(int nprob, int max_keys);
 // *nreused = columns with rep[k] != k
 cudaError_t launch_reuse_keys(const Problem& pb, int nprob, const ReuseTable& t, int32_t* rep,
                               int32_t* nreused, cudaStream_t st);
-cudaError_t launch_reuse_copy(const int32_t* rep, int nprob, const Output& out, cudaStream_t st);
+cudaError_t launch_reuse_copy(const int32_t* rep, int nprob, int bs, const Output& out,
+                              cudaStream_t st);
 
 // Adjoint of the setup (adjoint.cu): problem columns read their pattern and
 // solutions from the result M.

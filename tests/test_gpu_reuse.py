@@ -85,3 +85,28 @@ def test_adaptive_and_block_setups_ignore_the_table(h):
     M1, r1, _, _, stats = run(h, w.A, w.P, ep=0.4, ns=5, mn=5, ch=1)
     assert stats["reused_columns"] == 0
     assert bit_equal(M1, M0) and np.array_equal(r1, r0)
+
+
+@pytest.mark.parametrize("bs", [2, 3])
+@pytest.mark.parametrize("opt", [dict(ch=1), dict(cs=50)])
+def test_block_problems_reuse(h, bs, opt):
+    """Fixed block patterns: a constant-coefficient block stencil (the same
+    bs x bs blocks at every node of a 14 x 14 grid) has many identical block
+    problems; the block columns that take a representative's solution (its
+    values, its rows shifted by its block offset) give the M of the setup
+    without reuse, bit for bit."""
+    rng = np.random.default_rng(40 + bs)
+    Q = rng.standard_normal((bs, bs))
+    D = Q @ Q.T + 4.0 * np.eye(bs)
+    R = rng.standard_normal((bs, bs))
+    T = sp.diags([1.0, 1.0], [-1, 1], shape=(14, 14))
+    G = sp.kron(sp.identity(14), T) + sp.kron(T, sp.identity(14))
+    A = sp.csc_matrix(sp.kron(sp.identity(196), D) - 0.2 * sp.kron(G, R))
+    A.sort_indices()
+    P = mb.block_pattern(A, bs, "A")
+    M0, r0, s0, st0, _ = run(h, A, P, ns=0, bs=bs, prec="fp64")
+    M1, r1, s1, st1, stats = run(h, A, P, ns=0, bs=bs, prec="fp64", **opt)
+    assert bit_equal(M1, M0)
+    assert np.array_equal(r1.view(np.uint64), r0.view(np.uint64))
+    assert np.array_equal(st1, st0) and np.all(st1 == 0)
+    assert stats["reused_columns"] >= 100  # the interior nodes share one problem
