@@ -361,8 +361,9 @@ int mspai_setup(mspai_handle* h, const mspai_csc* C, const mspai_csc* C_rows, co
         return set_err(h, MSPAI_ERR_PARAM,
                        "Schur probing (-schur 1) is not supported by this setup: its target "
                        "[0; I; rho Be] and the n x N_p pattern are not built");
-    if (bs > 4)
-        return set_err(h, MSPAI_ERR_PARAM, "block size %d not supported (1..4)", bs);
+    if (bs > mspai::kMaxBlockSize)
+        return set_err(h, MSPAI_ERR_PARAM, "block size %d not supported (1..%d)", bs,
+                       mspai::kMaxBlockSize);
     if (n % bs != 0)
         return set_err(h, MSPAI_ERR_INPUT,
                        "block size %d does not divide the %d columns (constant blocks only)", bs,

@@ -619,12 +619,15 @@ __device__ double group_residual_gradient(const G& g, const Problem& pb, int col
     return g.sum(part);
 }
 
-// Solves the 3x3-or-smaller SPD system G Y = N (bs x bs, column-major) by
+// Largest constant block size of the block path.
+constexpr int kMaxBlockSize = 8;
+
+// Solves the bs x bs (bs <= kMaxBlockSize) SPD system G Y = N (column-major) by
 // Cholesky in FP64 and returns sum(Y .* N), the block rho term
 // <N, (A_j^T A_j)^-1 N> of Compute_Rhos_Block (src/Spai_Sub.imp:1350-1465).
 __device__ __forceinline__ double block_rho_term(double* Gm, const double* N, int bs)
 {
-    constexpr int kMaxBs = 4;
+    constexpr int kMaxBs = kMaxBlockSize;
     double L[kMaxBs * kMaxBs];
     for (int j = 0; j < bs; j++) {
         double d = Gm[j + j * bs];
@@ -883,7 +886,7 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
             // singleton rows, folded per column (one warp per column)
             for (int jj = g.warp(); jj < n; jj += G::kWarps) {
                 double sig = 0.0;
-                double tb[4] = {0.0, 0.0, 0.0, 0.0};
+                double tb[kMaxBlockSize] = {};
                 for (int e = s.off[jj] + lane; e < s.off[jj + 1]; e += 32) {
                     int u = 0;
                     const bool single =
@@ -893,7 +896,7 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
                         const double v = s.ev[e];
                         sig += v * v;
 #pragma unroll
-                        for (int c = 0; c < 4; c++)
+                        for (int c = 0; c < kMaxBlockSize; c++)
                             if (c < nrhs)
                                 tb[c] += v * (fixed ? s.r[static_cast<size_t>(c) * cap.emax + e]
                                                     : target_value(pb, bs * col + c, s.I[u]));
@@ -901,7 +904,7 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
                 }
                 sig = warp_sum(sig);
 #pragma unroll
-                for (int c = 0; c < 4; c++)
+                for (int c = 0; c < kMaxBlockSize; c++)
                     if (c < nrhs)
                         tb[c] = warp_sum(tb[c]);
                 if (lane == 0) {
@@ -1267,7 +1270,7 @@ __device__ void solve_column(const G& g, const Problem& pb, const Caps& cap, Slo
             }
             else {
                 // N = A_j(I)^T R (bs x bs), Gm = A_j^T A_j over the whole block column
-                double N[16], Gm[16];
+                double N[kMaxBlockSize * kMaxBlockSize], Gm[kMaxBlockSize * kMaxBlockSize];
                 for (int q = 0; q < bs * bs; q++)
                     N[q] = Gm[q] = 0.0;
                 for (int a = 0; a < bs; a++) {

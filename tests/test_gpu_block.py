@@ -90,3 +90,64 @@ def test_block_updates_with_target_rows(h):
     o = O.spai_block(C, sp.csc_matrix(Pb), 3, ns=3, mn=3, ep=0.05)
     assert same_pattern(M, o.M)
     assert max_rel_diff(M, o.M) < TOL["fp64"]
+
+
+def _block_stencil(nx, bs, seed):
+    """A 2-D 5-point block stencil on an nx x nx grid, random bs x bs blocks
+    per node (diagonal Q Q^T + 2 bs I, off-diagonal -R / 4)."""
+    rng = np.random.default_rng(seed)
+    nn = nx * nx
+    rows, cols, vals = [], [], []
+    for node in range(nn):
+        x, y = node % nx, node // nx
+        Q = rng.standard_normal((bs, bs))
+        blocks = [(node, Q @ Q.T + 2.0 * bs * np.eye(bs))]
+        for dx, dy in ((1, 0), (-1, 0), (0, 1), (0, -1)):
+            if 0 <= x + dx < nx and 0 <= y + dy < nx:
+                blocks.append((node + dx + dy * nx, -0.25 * rng.standard_normal((bs, bs))))
+        for nb, Bk in blocks:
+            for i in range(bs):
+                for j in range(bs):
+                    rows.append(bs * nb + i)
+                    cols.append(bs * node + j)
+                    vals.append(Bk[i, j])
+    A = sp.csc_matrix((vals, (rows, cols)), shape=(bs * nn, bs * nn))
+    A.sort_indices()
+    return A
+
+
+@pytest.mark.parametrize("bs", [5, 6, 8])
+@pytest.mark.parametrize("kind,kw,args", [
+    (-2, dict(ns=0), ["-2", "-1", "-ns", "0"]),
+    (-1, dict(ns=2, mn=2, ep=0.05), ["-1", "-1", "-ns", "2", "-mn", "2", "-ep", "0.05"]),
+])
+def test_block_sizes_up_to_8_against_reference(h, tmp_path, bs, kind, kw, args):
+    """Constant block sizes 5, 6 and 8: the GPU's M equals the reference's
+    own block run (oracle/_ref/ref_driver -bs k) in FP64 to 1e-10 per entry
+    (the reference prints 14 digits)."""
+    import os
+    import subprocess
+    from fullsize import REF_DRIVER, read_mm, write_mm
+    if not os.path.exists(REF_DRIVER):
+        pytest.skip("oracle/_ref/ref_driver was not built")
+    A = _block_stencil(6, bs, seed=bs)
+    write_mm(str(tmp_path / "A.mtx"), A)
+    r = subprocess.run([REF_DRIVER, "A.mtx"] + args + ["-bs", str(bs), "-out", "ref.mtx"],
+                       cwd=str(tmp_path), capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-1000:]
+    ref = read_mm(str(tmp_path / "ref.mtx"))
+    Pb = mb.block_pattern(A, bs, kind)
+    h.setup(A, Pb, options=mb.Options(bs=bs, prec="fp64", **kw))
+    M = h.result()
+    _, steps, status = h.column_info()
+    assert np.all(status == 0)
+    assert same_pattern(M, ref)
+    assert max_rel_diff(M, ref) < max(TOL["fp64"], PRINT_TOL)
+    if kind == -1:
+        assert steps.max() > 1  # the block patterns grew
+
+
+def test_block_size_above_8_refused(h):
+    A = sp.identity(90, format="csc")
+    with pytest.raises(mb.MspaiError, match="block size"):
+        h.setup(A, sp.identity(10, format="csc"), options=mb.Options(bs=9, ns=0))
