@@ -1393,8 +1393,10 @@ __device__ bool fixed_solve_column(const CtaGroup<NT>& g, FixShared<T>& fs, cons
         const int nblk = (n + kFixPanel - 1) / kFixPanel;
         T* gv = b2.low<T>(n);
         T* Gs = b2.low<T>(r_el);
-        T* tile = b2.low<T>(kFixPanel * n);
-        T* Dr = b2.low<T>(kFixPanel * kFixPanel * nblk);
+        // the tile is dead once the factorization ends: the inverted diagonal
+        // blocks take its place
+        T* tile = b2.low<T>(max(kFixPanel * n, kFixPanel * kFixPanel * nblk));
+        T* Dr = tile;
         if (b2.ok()) {
             // G = C^T C: column j of G's lower triangle (= row j of its upper
             // triangle, packed as R) by one thread, in entry order
