@@ -726,103 +726,109 @@ __device__ void fix_forward_substitute(const CtaGroup<NT>& g, const T* R, int n,
     }
 }
 
+// Warp-level factorization of the 16 x 16 diagonal block at c0 (nb rows) in
+// place; returns true (on every lane) when a pivot is not positive.
+template <class T>
+__device__ __forceinline__ bool fix_chol_diag(T* R, int n, int c0, int nb, int lane)
+{
+    T a[kFixPanel];
+#pragma unroll
+    for (int j = 0; j < kFixPanel; j++)
+        a[j] = (lane < nb && j >= lane && j < nb) ? R[fix_rs(c0 + lane, n) + (j - lane)] : T(0);
+    bool bad = false;
+#pragma unroll
+    for (int k = 0; k < kFixPanel; k++) {
+        if (k < nb) {
+            const T piv = __shfl_sync(0xffffffffu, a[k], k);
+            bad = bad || !(piv > T(0));
+            const T rkk = bad ? T(1) : sqrt(piv);
+            const T inv = T(1) / rkk;
+            if (lane == k) {
+#pragma unroll
+                for (int j = 0; j < kFixPanel; j++)
+                    a[j] = (j == k) ? rkk : (j > k ? a[j] * inv : a[j]);
+            }
+            T rk[kFixPanel];
+#pragma unroll
+            for (int j = 0; j < kFixPanel; j++)
+                rk[j] = __shfl_sync(0xffffffffu, a[j], k);
+            if (lane > k && lane < nb) {
+#pragma unroll
+                for (int j = 0; j < kFixPanel; j++)
+                    if (j >= lane)
+                        a[j] -= rk[lane] * rk[j];
+            }
+        }
+    }
+    if (lane < nb) {
+#pragma unroll
+        for (int j = 0; j < kFixPanel; j++)
+            if (j >= lane && j < nb)
+                R[fix_rs(c0 + lane, n) + (j - lane)] = a[j];
+    }
+    return bad;
+}
+
 // Cholesky factorization G = R^T R in place, R upper triangular in the packed
 // rows of fix_rs (row i holds columns i .. n - 1 of G's upper triangle on
-// entry, of R on return).  Right-looking by 16 columns: warp 0 factors the
-// diagonal block in registers (no CTA barrier inside); a thread per later
-// column solves R11^T X = G12 for its 16 entries; the trailing upper
-// triangle is updated by a thread per column.  Three barriers per block.
-// Returns false (uniformly) when a pivot is not positive (G not numerically
-// positive definite in T).  tile: 16 n elements, 16-byte aligned (the block
-// row of R right of the diagonal block, 16 consecutive values per column).
+// entry, of R on return).  Right-looking by 16 columns with look-ahead: a
+// thread per later column solves R11^T X = G12 for its 16 entries of the
+// block row; the trailing update of the next block row runs first (a thread
+// per column); then warp 0 factors the next diagonal block in registers while
+// the other warps update the rows below it.  Three barriers per block, and
+// the diagonal factorization off the critical path while the trailing
+// triangle is large.  Every element of G sees the same operations in the same
+// order as in the plain right-looking order.  Returns false (uniformly) when
+// a pivot is not positive (G not numerically positive definite in T).
+// tile: 16 n elements, 16-byte aligned (the block row of R right of the
+// diagonal block, 16 consecutive values per column).
 template <class T, int NT>
 __device__ bool fix_cholesky(const CtaGroup<NT>& g, FixShared<T>& fs, T* R, int n, T* tile)
 {
+    static_assert(NT > 32, "the look-ahead needs warps besides warp 0");
     const int tid = threadIdx.x, lane = tid & 31;
-    if (tid == 0)
-        fs.chol_fail = 0;
+    if (tid < 32) {
+        const bool bad = fix_chol_diag<T>(R, n, 0, min(kFixPanel, n), lane);
+        if (lane == 0)
+            fs.chol_fail = bad ? 1 : 0;
+    }
     g.sync();
-    for (int c0 = 0; c0 < n; c0 += kFixPanel) {
-        const int nb = min(kFixPanel, n - c0);
-        if (tid < 32) {
-            // lane i < nb holds row c0 + i of the diagonal block (columns >= i)
-            T a[kFixPanel];
-#pragma unroll
-            for (int j = 0; j < kFixPanel; j++)
-                a[j] = (lane < nb && j >= lane && j < nb) ? R[fix_rs(c0 + lane, n) + (j - lane)]
-                                                          : T(0);
-            bool bad = false;
-#pragma unroll
-            for (int k = 0; k < kFixPanel; k++) {
-                if (k < nb) {
-                    const T piv = __shfl_sync(0xffffffffu, a[k], k);
-                    bad = bad || !(piv > T(0));
-                    const T rkk = bad ? T(1) : sqrt(piv);
-                    const T inv = T(1) / rkk;
-                    if (lane == k) {
-#pragma unroll
-                        for (int j = 0; j < kFixPanel; j++)
-                            a[j] = (j == k) ? rkk : (j > k ? a[j] * inv : a[j]);
-                    }
-                    // row k of R, broadcast; rows below subtract its outer product
-                    T rk[kFixPanel];
-#pragma unroll
-                    for (int j = 0; j < kFixPanel; j++)
-                        rk[j] = __shfl_sync(0xffffffffu, a[j], k);
-                    if (lane > k && lane < nb) {
-#pragma unroll
-                        for (int j = 0; j < kFixPanel; j++)
-                            if (j >= lane)
-                                a[j] -= rk[lane] * rk[j];
-                    }
-                }
-            }
-            if (lane < nb) {
-#pragma unroll
-                for (int j = 0; j < kFixPanel; j++)
-                    if (j >= lane && j < nb)
-                        R[fix_rs(c0 + lane, n) + (j - lane)] = a[j];
-            }
-            if (lane == 0 && bad)
-                fs.chol_fail = 1;
-        }
-        g.sync();
-        if (fs.chol_fail)
-            return false;  // uniform: read after the barrier
+    if (fs.chol_fail)
+        return false;
+    for (int c0 = 0; c0 + kFixPanel < n; c0 += kFixPanel) {
+        const int nb = kFixPanel;  // every block but the last is full
         const int c1 = c0 + nb;
         // R(c0:c1, j) for j >= c1: forward substitution with R11^T, one column per thread
         for (int j = c1 + tid; j < n; j += NT) {
             T x[kFixPanel];
 #pragma unroll
             for (int i = 0; i < kFixPanel; i++) {
-                if (i < nb) {
-                    const T* ri = R + fix_rs(c0 + i, n) - (c0 + i);  // ri[c] = R(c0 + i, c)
-                    T v = ri[j];
+                const T* ri = R + fix_rs(c0 + i, n) - (c0 + i);  // ri[c] = R(c0 + i, c)
+                T v = ri[j];
 #pragma unroll
-                    for (int l = 0; l < kFixPanel; l++)
-                        if (l < i)
-                            v -= R[fix_rs(c0 + l, n) + (c0 + i - c0 - l)] * x[l];
-                    x[i] = v / ri[c0 + i];
-                }
+                for (int l = 0; l < kFixPanel; l++)
+                    if (l < i)
+                        v -= R[fix_rs(c0 + l, n) + (c0 + i - c0 - l)] * x[l];
+                x[i] = v / ri[c0 + i];
             }
             T* tj = tile + static_cast<size_t>(j - c1) * kFixPanel;
 #pragma unroll
             for (int i = 0; i < kFixPanel; i++) {
-                if (i < nb)
-                    R[fix_rs(c0 + i, n) + (j - c0 - i)] = x[i];
-                tj[i] = (i < nb) ? x[i] : T(0);
+                R[fix_rs(c0 + i, n) + (j - c0 - i)] = x[i];
+                tj[i] = x[i];
             }
         }
         g.sync();
-        // trailing update G(i, j) -= sum_l R(c0 + l, i) R(c0 + l, j), c1 <= i <= j < n;
-        // a thread per column j keeps R(c0 + l, j) in registers, column i's 16
-        // values come from the tile (broadcast: the threads of a warp are at
-        // the same i)
+        const int nb2 = min(kFixPanel, n - c1);
+        const int c2 = c1 + nb2;
+        // trailing update of the next block row: G(i, j) -= sum_l R(c0 + l, i) R(c0 + l, j),
+        // c1 <= i < c2, i <= j < n
         for (int j = c1 + tid; j < n; j += NT) {
             T rj[kFixPanel];
             fix_load16(tile + static_cast<size_t>(j - c1) * kFixPanel, rj);
-            T* gj = R + j;  // gj[fix_rs(i, n) - i] = G(i, j)
-            for (int i = c1; i <= j; i++) {
+            T* gj = R + j;
+            const int iend = min(j, c2 - 1);
+            for (int i = c1; i <= iend; i++) {
                 T v[kFixPanel];
                 fix_load16(tile + static_cast<size_t>(i - c1) * kFixPanel, v);
                 T s0 = T(0), s1 = T(0);
@@ -835,6 +841,33 @@ __device__ bool fix_cholesky(const CtaGroup<NT>& g, FixShared<T>& fs, T* R, int 
             }
         }
         g.sync();
+        if (tid < 32) {
+            // the next diagonal block is final: factor it
+            const bool bad = fix_chol_diag<T>(R, n, c1, nb2, lane);
+            if (lane == 0 && bad)
+                fs.chol_fail = 1;
+        } else {
+            // ... while the other warps update the rows below it
+            for (int j = c2 + tid - 32; j < n; j += NT - 32) {
+                T rj[kFixPanel];
+                fix_load16(tile + static_cast<size_t>(j - c1) * kFixPanel, rj);
+                T* gj = R + j;
+                for (int i = c2; i <= j; i++) {
+                    T v[kFixPanel];
+                    fix_load16(tile + static_cast<size_t>(i - c1) * kFixPanel, v);
+                    T s0 = T(0), s1 = T(0);
+#pragma unroll
+                    for (int l = 0; l < kFixPanel; l += 2) {
+                        s0 += v[l] * rj[l];
+                        s1 += v[l + 1] * rj[l + 1];
+                    }
+                    gj[fix_rs(i, n) - i] -= s0 + s1;
+                }
+            }
+        }
+        g.sync();
+        if (fs.chol_fail)
+            return false;
     }
     return true;
 }
