@@ -83,6 +83,7 @@ struct FixShared {
     int nspec;
     int mcount;                     // distinct rows of C(:, J)
     int chol_fail;                  // a pivot of the Cholesky factorization was not positive
+    T chol_rdiag[16];               // 1 / R(i, i) of the Cholesky's current diagonal block
     int spec_e[kFixMaxSpecial];
     int spec_jj[kFixMaxSpecial];
     double spec_v[kFixMaxSpecial];
@@ -727,9 +728,10 @@ __device__ void fix_forward_substitute(const CtaGroup<NT>& g, const T* R, int n,
 }
 
 // Warp-level factorization of the 16 x 16 diagonal block at c0 (nb rows) in
-// place; returns true (on every lane) when a pivot is not positive.
+// place, the reciprocals of its diagonal into rdiag; returns true (on every
+// lane) when a pivot is not positive.
 template <class T>
-__device__ __forceinline__ bool fix_chol_diag(T* R, int n, int c0, int nb, int lane)
+__device__ __forceinline__ bool fix_chol_diag(T* R, int n, int c0, int nb, int lane, T* rdiag)
 {
     T a[kFixPanel];
 #pragma unroll
@@ -744,6 +746,7 @@ __device__ __forceinline__ bool fix_chol_diag(T* R, int n, int c0, int nb, int l
             const T rkk = bad ? T(1) : sqrt(piv);
             const T inv = T(1) / rkk;
             if (lane == k) {
+                rdiag[k] = inv;
 #pragma unroll
                 for (int j = 0; j < kFixPanel; j++)
                     a[j] = (j == k) ? rkk : (j > k ? a[j] * inv : a[j]);
@@ -788,7 +791,7 @@ __device__ bool fix_cholesky(const CtaGroup<NT>& g, FixShared<T>& fs, T* R, int 
     static_assert(NT > 32, "the look-ahead needs warps besides warp 0");
     const int tid = threadIdx.x, lane = tid & 31;
     if (tid < 32) {
-        const bool bad = fix_chol_diag<T>(R, n, 0, min(kFixPanel, n), lane);
+        const bool bad = fix_chol_diag<T>(R, n, 0, min(kFixPanel, n), lane, fs.chol_rdiag);
         if (lane == 0)
             fs.chol_fail = bad ? 1 : 0;
     }
@@ -798,7 +801,8 @@ __device__ bool fix_cholesky(const CtaGroup<NT>& g, FixShared<T>& fs, T* R, int 
     for (int c0 = 0; c0 + kFixPanel < n; c0 += kFixPanel) {
         const int nb = kFixPanel;  // every block but the last is full
         const int c1 = c0 + nb;
-        // R(c0:c1, j) for j >= c1: forward substitution with R11^T, one column per thread
+        // R(c0:c1, j) for j >= c1: forward substitution with R11^T (the diagonal
+        // as reciprocals from the factor step), one column per thread
         for (int j = c1 + tid; j < n; j += NT) {
             T x[kFixPanel];
 #pragma unroll
@@ -809,7 +813,7 @@ __device__ bool fix_cholesky(const CtaGroup<NT>& g, FixShared<T>& fs, T* R, int 
                 for (int l = 0; l < kFixPanel; l++)
                     if (l < i)
                         v -= R[fix_rs(c0 + l, n) + (c0 + i - c0 - l)] * x[l];
-                x[i] = v / ri[c0 + i];
+                x[i] = v * fs.chol_rdiag[i];
             }
             T* tj = tile + static_cast<size_t>(j - c1) * kFixPanel;
 #pragma unroll
@@ -843,7 +847,7 @@ __device__ bool fix_cholesky(const CtaGroup<NT>& g, FixShared<T>& fs, T* R, int 
         g.sync();
         if (tid < 32) {
             // the next diagonal block is final: factor it
-            const bool bad = fix_chol_diag<T>(R, n, c1, nb2, lane);
+            const bool bad = fix_chol_diag<T>(R, n, c1, nb2, lane, fs.chol_rdiag);
             if (lane == 0 && bad)
                 fs.chol_fail = 1;
         } else {
