@@ -728,10 +728,12 @@ __device__ void fix_forward_substitute(const CtaGroup<NT>& g, const T* R, int n,
 }
 
 // Warp-level factorization of the 16 x 16 diagonal block at c0 (nb rows) in
-// place, the reciprocals of its diagonal into rdiag; returns true (on every
-// lane) when a pivot is not positive.
+// place, the reciprocals of its diagonal into rdiag and the factored block
+// into r11 (16 x 16 row-major, zero below the diagonal); returns true (on
+// every lane) when a pivot is not positive.
 template <class T>
-__device__ __forceinline__ bool fix_chol_diag(T* R, int n, int c0, int nb, int lane, T* rdiag)
+__device__ __forceinline__ bool fix_chol_diag(T* R, int n, int c0, int nb, int lane, T* rdiag,
+                                              T* r11)
 {
     T a[kFixPanel];
 #pragma unroll
@@ -769,6 +771,11 @@ __device__ __forceinline__ bool fix_chol_diag(T* R, int n, int c0, int nb, int l
             if (j >= lane && j < nb)
                 R[fix_rs(c0 + lane, n) + (j - lane)] = a[j];
     }
+    if (lane < kFixPanel) {
+#pragma unroll
+        for (int j = 0; j < kFixPanel; j++)
+            r11[lane * kFixPanel + j] = a[j];
+    }
     return bad;
 }
 
@@ -784,14 +791,16 @@ __device__ __forceinline__ bool fix_chol_diag(T* R, int n, int c0, int nb, int l
 // order as in the plain right-looking order.  Returns false (uniformly) when
 // a pivot is not positive (G not numerically positive definite in T).
 // tile: 16 n elements, 16-byte aligned (the block row of R right of the
-// diagonal block, 16 consecutive values per column).
+// diagonal block, 16 consecutive values per column); r11: 256 elements,
+// 16-byte aligned (the current diagonal block of R, dense).
 template <class T, int NT>
-__device__ bool fix_cholesky(const CtaGroup<NT>& g, FixShared<T>& fs, T* R, int n, T* tile)
+__device__ bool fix_cholesky(const CtaGroup<NT>& g, FixShared<T>& fs, T* R, int n, T* tile,
+                             T* r11)
 {
     static_assert(NT > 32, "the look-ahead needs warps besides warp 0");
     const int tid = threadIdx.x, lane = tid & 31;
     if (tid < 32) {
-        const bool bad = fix_chol_diag<T>(R, n, 0, min(kFixPanel, n), lane, fs.chol_rdiag);
+        const bool bad = fix_chol_diag<T>(R, n, 0, min(kFixPanel, n), lane, fs.chol_rdiag, r11);
         if (lane == 0)
             fs.chol_fail = bad ? 1 : 0;
     }
@@ -801,19 +810,25 @@ __device__ bool fix_cholesky(const CtaGroup<NT>& g, FixShared<T>& fs, T* R, int 
     for (int c0 = 0; c0 + kFixPanel < n; c0 += kFixPanel) {
         const int nb = kFixPanel;  // every block but the last is full
         const int c1 = c0 + nb;
-        // R(c0:c1, j) for j >= c1: forward substitution with R11^T (the diagonal
-        // as reciprocals from the factor step), one column per thread
+        // R(c0:c1, j) for j >= c1: forward substitution with R11^T, one column
+        // per thread, R11 row by row from the dense copy (broadcast 16-byte
+        // loads) and its diagonal as reciprocals from the factor step; each
+        // entry takes its terms in the order l = 0, 1, ... as a column-wise
+        // substitution would
         for (int j = c1 + tid; j < n; j += NT) {
             T x[kFixPanel];
 #pragma unroll
-            for (int i = 0; i < kFixPanel; i++) {
-                const T* ri = R + fix_rs(c0 + i, n) - (c0 + i);  // ri[c] = R(c0 + i, c)
-                T v = ri[j];
+            for (int i = 0; i < kFixPanel; i++)
+                x[i] = R[fix_rs(c0 + i, n) + (j - c0 - i)];
 #pragma unroll
-                for (int l = 0; l < kFixPanel; l++)
-                    if (l < i)
-                        v -= R[fix_rs(c0 + l, n) + (c0 + i - c0 - l)] * x[l];
-                x[i] = v * fs.chol_rdiag[i];
+            for (int l = 0; l < kFixPanel; l++) {
+                x[l] = x[l] * fs.chol_rdiag[l];
+                T rl[kFixPanel];
+                fix_load16(r11 + l * kFixPanel, rl);
+#pragma unroll
+                for (int i = 0; i < kFixPanel; i++)
+                    if (i > l)
+                        x[i] -= rl[i] * x[l];
             }
             T* tj = tile + static_cast<size_t>(j - c1) * kFixPanel;
 #pragma unroll
@@ -847,7 +862,7 @@ __device__ bool fix_cholesky(const CtaGroup<NT>& g, FixShared<T>& fs, T* R, int 
         g.sync();
         if (tid < 32) {
             // the next diagonal block is final: factor it
-            const bool bad = fix_chol_diag<T>(R, n, c1, nb2, lane, fs.chol_rdiag);
+            const bool bad = fix_chol_diag<T>(R, n, c1, nb2, lane, fs.chol_rdiag, r11);
             if (lane == 0 && bad)
                 fs.chol_fail = 1;
         } else {
@@ -1434,6 +1449,7 @@ __device__ bool fixed_solve_column(const CtaGroup<NT>& g, FixShared<T>& fs, cons
         // blocks take its place
         T* tile = b2.low<T>(max(kFixPanel * n, kFixPanel * kFixPanel * nblk));
         T* Dr = tile;
+        T* r11 = b2.low<T>(kFixPanel * kFixPanel);  // the current diagonal block
         if (b2.ok()) {
             // G = C^T C: column j of G's lower triangle (= row j of its upper
             // triangle, packed as R) by one thread, in entry order
@@ -1461,7 +1477,7 @@ __device__ bool fixed_solve_column(const CtaGroup<NT>& g, FixShared<T>& fs, cons
             }
             g.sync();
             PHASE_MARK(2);
-            const bool factored = fix_cholesky<T, NT>(g, fs, Gs, n, tile);
+            const bool factored = fix_cholesky<T, NT>(g, fs, Gs, n, tile, r11);
             PHASE_MARK(3);
             if (factored) {
                 fix_invert_diag<T, NT>(Gs, n, Dr);
